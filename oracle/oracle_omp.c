@@ -1,0 +1,44 @@
+/*
+ * TEST INFRASTRUCTURE ONLY: the timed CPU baseline.
+ *
+ * Runs the oracle the way the reference's own benchmark drives its library
+ * (skel/test/benchmark_eri.cpp:135-216): one multi-shell-pair per bra shell
+ * pair, the whole ket list as Q, OpenMP dynamic scheduling over the bra
+ * pairs, every thread with its own output buffer.
+ */
+#include <omp.h>
+#include <stdlib.h>
+#include "simint/shell/shell.h"
+
+int oracle_compute_eri(struct simint_multi_shellpair const * P,
+                       struct simint_multi_shellpair const * Q,
+                       double screen_tol, int deriv, int ordering, double * out);
+
+/* Returns wall seconds; out_checksum receives the sum of all outputs. */
+double oracle_bench_omp(int nbra, struct simint_multi_shellpair const * Plist,
+                        struct simint_multi_shellpair const * Q,
+                        double screen_tol, int deriv, int nthreads, int nout_per_bra,
+                        double * out_checksum)
+{
+    if(nthreads > 0)
+        omp_set_num_threads(nthreads);
+    double total = 0.0;
+    const double t0 = omp_get_wtime();
+    #pragma omp parallel reduction(+:total)
+    {
+        double * buf = (double *)malloc(sizeof(double) * (size_t)nout_per_bra);
+        #pragma omp for schedule(dynamic)
+        for(int b = 0; b < nbra; b++)
+        {
+            int r = oracle_compute_eri(&Plist[b], Q, screen_tol, deriv, 0, buf);
+            if(r > 0)
+                for(int k = 0; k < nout_per_bra; k++)
+                    total += buf[k];
+        }
+        free(buf);
+    }
+    const double t1 = omp_get_wtime();
+    if(out_checksum)
+        *out_checksum = total;
+    return t1 - t0;
+}

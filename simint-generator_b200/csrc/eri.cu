@@ -1,0 +1,587 @@
+// Host runtime of the B200 Simint engine: simint_init/finalize,
+// simint_compute_eri(_deriv) and the run-time dispatch to the generated
+// per-class kernels.
+//
+// Reference behaviour kept (skel/simint/ostei/ostei.c:10-41,
+// skel/simint/simint_eri.c:4-22): the tolerance is squared, a pair-level
+// test returns -1 without writing when P.screen_max*Q.screen_max < tol^2,
+// the result count is nshell12_clip(P)*nshell12_clip(Q), output is
+// bra-pair-major then Cartesian a,b,c,d row major.
+//
+// Everything else is B200-specific: the pair SoA is packed into 128-byte
+// primitive records, uploaded with one copy per pair set, one thread
+// computes one shell quartet, kets are visited in order of primitive count,
+// and the result comes back with one device-to-host copy.
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "simint/simint.h"
+#include "simint_b200.h"
+#include "kernels.h"
+#include "runtime.h"
+#include "gen/boys_grid.inc"
+
+namespace sb200 {
+
+static std::mutex g_mutex;
+static bool g_initialised = false;
+static int g_ordering = SIMINT_B200_ORDERING_PSI4;
+static int g_precision = SIMINT_B200_PREC_FP64;
+static double g_gate = 0.0;
+static KernelTable g_table;
+static std::map<std::array<int, 4>, int> g_unique;     // unique class -> index in g_table
+static std::vector<double *> g_boys_dev;              // per device: Boys tables
+static thread_local std::string t_last_error;
+static thread_local long long t_launches = 0;
+
+void set_error(const std::string & s)
+{
+    t_last_error = s;
+}
+
+void count_launch(long long n) { t_launches += n; }
+
+static int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+int ncart_of(int l) { return ncart(l); }
+
+// Psi4 position of (i,j,k) inside its shell
+static int psi4_index(int i, int j, int k)
+{
+    const int l = i + j + k;
+    (void)j;
+    return ((l - i) * (l - i + 1)) / 2 + k;
+}
+
+int cart_index(int i, int j, int k, int ordering)
+{
+    const int l = i + j + k;
+    if(ordering == SIMINT_B200_ORDERING_GAMESS && (l == 2 || l == 3))
+    {
+        // generator/Ordering_GAMESS.cpp:20-41
+        static const int g2[6][3] = {{2,0,0},{0,2,0},{0,0,2},{1,1,0},{1,0,1},{0,1,1}};
+        static const int g3[10][3] = {{3,0,0},{0,3,0},{0,0,3},{2,1,0},{2,0,1},
+                                      {1,2,0},{0,2,1},{1,0,2},{0,1,2},{1,1,1}};
+        const int n = ncart(l);
+        for(int t = 0; t < n; t++)
+        {
+            const int * g = (l == 2) ? g2[t] : g3[t];
+            if(g[0] == i && g[1] == j && g[2] == k)
+                return t;
+        }
+    }
+    return psi4_index(i, j, k);
+}
+
+void carts(int l, std::vector<std::array<int, 3>> & out)
+{
+    out.clear();
+    for(int i = l; i >= 0; i--)
+        for(int j = l - i; j >= 0; j--)
+            out.push_back({i, j, l - i - j});
+}
+
+UniqueMap unique_of(const int am[4])
+{
+    // emit.unique_class: canonical (a>=b, c>=d, (a+b, a) >= (c+d, c))
+    UniqueMap u;
+    int a = am[0], b = am[1], c = am[2], d = am[3];
+    int sb = a < b, sk = c < d;
+    if(sb) std::swap(a, b);
+    if(sk) std::swap(c, d);
+    int pq = (a + b < c + d) || (a + b == c + d && a < c);
+    if(pq)
+    {
+        std::swap(a, c);
+        std::swap(b, d);
+        std::swap(sb, sk);
+    }
+    u.am[0] = a; u.am[1] = b; u.am[2] = c; u.am[3] = d;
+    u.swapB = sb; u.swapK = sk; u.pq = pq;
+    return u;
+}
+
+// Output index table: for the unique class element n (Psi4 order), the
+// position inside the requested class's shell-quartet block.
+std::vector<unsigned short> make_oidx(const int req[4], const UniqueMap & u, int ordering)
+{
+    std::vector<std::array<int, 3>> ca, cb, cc, cd;
+    carts(u.am[0], ca); carts(u.am[1], cb); carts(u.am[2], cc); carts(u.am[3], cd);
+    std::vector<unsigned short> o;
+    o.reserve(ca.size() * cb.size() * cc.size() * cd.size());
+    for(auto & gA : ca) for(auto & gB : cb) for(auto & gC : cc) for(auto & gD : cd)
+    {
+        std::array<int, 3> b0 = u.swapB ? gB : gA, b1 = u.swapB ? gA : gB;
+        std::array<int, 3> k0 = u.swapK ? gD : gC, k1 = u.swapK ? gC : gD;
+        std::array<int, 3> p0, p1, q0, q1;
+        if(!u.pq) { p0 = b0; p1 = b1; q0 = k0; q1 = k1; }
+        else      { q0 = b0; q1 = b1; p0 = k0; p1 = k1; }
+        const int i0 = cart_index(p0[0], p0[1], p0[2], ordering);
+        const int i1 = cart_index(p1[0], p1[1], p1[2], ordering);
+        const int i2 = cart_index(q0[0], q0[1], q0[2], ordering);
+        const int i3 = cart_index(q1[0], q1[1], q1[2], ordering);
+        o.push_back((unsigned short)(((i0 * ncart(req[1]) + i1) * ncart(req[2]) + i2) * ncart(req[3]) + i3));
+    }
+    return o;
+}
+
+const ClassKernels * find_kernels(const UniqueMap & u)
+{
+    auto it = g_unique.find({u.am[0], u.am[1], u.am[2], u.am[3]});
+    if(it == g_unique.end())
+        return nullptr;
+    return &g_table.list[it->second];
+}
+
+int ensure_device()
+{
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess)
+    {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        return -1;
+    }
+    int ndev = 0;
+    if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+    {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if((int)g_boys_dev.size() < ndev)
+        g_boys_dev.resize(ndev, nullptr);
+    if(!g_boys_dev[dev])
+    {
+        double * d = nullptr;
+        const size_t n1 = sizeof(simint_b200_boys_grid_host), n2 = sizeof(simint_b200_boys_longfac_host);
+        if(cudaMalloc(&d, n1 + n2) != cudaSuccess ||
+           cudaMemcpy(d, simint_b200_boys_grid_host, n1, cudaMemcpyHostToDevice) != cudaSuccess ||
+           cudaMemcpy((char *)d + n1, simint_b200_boys_longfac_host, n2, cudaMemcpyHostToDevice) != cudaSuccess)
+        {
+            set_error(std::string("Boys table upload failed: ") + cudaGetErrorString(cudaGetLastError()));
+            return -1;
+        }
+        g_boys_dev[dev] = d;
+    }
+    return dev;
+}
+
+const double * boys_table()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mutex);
+    return dev < (int)g_boys_dev.size() ? g_boys_dev[dev] : nullptr;
+}
+
+int ordering() { return g_ordering; }
+int precision() { return g_precision; }
+double gate() { return g_gate; }
+
+void init_tables()
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if(g_initialised)
+        return;
+    simint_b200_register_generated(g_table);
+    for(size_t k = 0; k < g_table.list.size(); k++)
+    {
+        const auto & e = g_table.list[k];
+        g_unique[{e.am[0], e.am[1], e.am[2], e.am[3]}] = (int)k;
+    }
+    const char * o = getenv("SIMINT_B200_ORDERING");
+    if(o && (!strcmp(o, "gamess") || !strcmp(o, "GAMESS") || !strcmp(o, "1")))
+        g_ordering = SIMINT_B200_ORDERING_GAMESS;
+    g_initialised = true;
+}
+
+// ---------------------------------------------------------------------
+// Per-thread device workspace (grow-only)
+// ---------------------------------------------------------------------
+
+Workspace & workspace()
+{
+    static thread_local Workspace w;
+    return w;
+}
+
+bool DevBuf::reserve(size_t n)
+{
+    if(n <= cap)
+        return true;
+    if(ptr)
+        cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t want = std::max(n, (size_t)4096);
+    want = (want * 5) / 4;
+    if(cudaMalloc(&ptr, want) != cudaSuccess)
+    {
+        cudaGetLastError();
+        ptr = nullptr;
+        return false;
+    }
+    cap = want;
+    return true;
+}
+
+void DevBuf::release()
+{
+    if(ptr)
+        cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+bool HostBuf::reserve(size_t n)
+{
+    if(n <= cap)
+        return true;
+    if(ptr)
+        cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t want = (std::max(n, (size_t)4096) * 5) / 4;
+    if(cudaMallocHost(&ptr, want) != cudaSuccess)
+    {
+        cudaGetLastError();
+        ptr = nullptr;
+        return false;
+    }
+    cap = want;
+    return true;
+}
+
+void HostBuf::release()
+{
+    if(ptr)
+        cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+Workspace::~Workspace()
+{
+    // device buffers are released by simint_finalize on the owning thread;
+    // at process exit the driver reclaims them.
+}
+
+// Padded slot layout of a multi-shell-pair (shell.c:538-570): after every
+// 16 shell pairs the slot index is rounded up to a multiple of 8.
+void pair_starts(const simint_multi_shellpair * P, std::vector<int> & start, int & npad)
+{
+    start.resize(P->nshell12);
+    int idx = 0;
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        start[p] = idx;
+        idx += P->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 || p + 1 >= P->nshell12)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    npad = idx;
+}
+
+// Pack one pair set into host staging memory: records, starts, counts, AB.
+size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L)
+{
+    std::vector<int> start;
+    int npad = 0;
+    pair_starts(P, start, npad);
+    L.npad = npad;
+    L.npair = P->nshell12;
+    L.off_rec = 0;
+    L.off_start = (size_t)npad * SB_REC * sizeof(double);
+    L.off_nprim = L.off_start + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    L.off_AB = L.off_nprim + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    const size_t total = L.off_AB + 3 * (size_t)P->nshell12 * sizeof(double);
+    if(!dst)
+        return total;
+    double * rec = (double *)(dst + L.off_rec);
+    const bool has_screen = P->screen != nullptr;
+    for(int s = 0; s < npad; s++)
+    {
+        double * r = rec + (size_t)s * SB_REC;
+        r[0] = P->alpha[s]; r[1] = P->prefac[s];
+        r[2] = P->x[s]; r[3] = P->y[s]; r[4] = P->z[s];
+        r[5] = P->PA_x[s]; r[6] = P->PA_y[s]; r[7] = P->PA_z[s];
+        r[8] = P->PB_x[s]; r[9] = P->PB_y[s]; r[10] = P->PB_z[s];
+        r[11] = P->alpha2 ? P->alpha2[s] : 0.0;
+        r[12] = P->beta2 ? P->beta2[s] : 0.0;
+        const double sc = has_screen ? P->screen[s] : 0.0;
+        r[13] = sc;
+        r[15] = has_screen ? std::sqrt(std::max(sc, 0.0)) : INFINITY;
+    }
+    for(int g = 0; g < npad; g += 8)
+    {
+        double m = 0.0;
+        for(int s = g; s < std::min(g + 8, npad); s++)
+            m = std::max(m, rec[(size_t)s * SB_REC + 13]);
+        for(int s = g; s < std::min(g + 8, npad); s++)
+            rec[(size_t)s * SB_REC + 14] = m;
+    }
+    memcpy(dst + L.off_start, start.data(), P->nshell12 * sizeof(int));
+    memcpy(dst + L.off_nprim, P->nprim12, P->nshell12 * sizeof(int));
+    double * ab = (double *)(dst + L.off_AB);
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        ab[3 * p + 0] = P->AB_x[p];
+        ab[3 * p + 1] = P->AB_y[p];
+        ab[3 * p + 2] = P->AB_z[p];
+    }
+    return total;
+}
+
+PairSetDev device_view(const char * base, const PackedLayout & L, double screen_max)
+{
+    PairSetDev d;
+    d.prim = (const double *)(base + L.off_rec);
+    d.pstart = (const int *)(base + L.off_start);
+    d.nprim = (const int *)(base + L.off_nprim);
+    d.AB = (const double *)(base + L.off_AB);
+    d.screen_max = screen_max;
+    d.npair = L.npair;
+    return d;
+}
+
+// Device copy of an output-index table, cached per (device, class, variant).
+const unsigned short * oidx_table(const int req[4], const UniqueMap & u, int ord)
+{
+    static std::mutex m;
+    static std::map<std::array<int, 7>, unsigned short *> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::array<int, 7> key = {dev, req[0], req[1], req[2], req[3], ord, 0};
+    std::lock_guard<std::mutex> lk(m);
+    auto it = cache.find(key);
+    if(it != cache.end())
+        return it->second;
+    std::vector<unsigned short> h = make_oidx(req, u, ord);
+    unsigned short * d = nullptr;
+    if(cudaMalloc(&d, h.size() * sizeof(unsigned short)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaMemcpy(d, h.data(), h.size() * sizeof(unsigned short), cudaMemcpyHostToDevice);
+    cache[key] = d;
+    return d;
+}
+
+} // namespace sb200
+
+using namespace sb200;
+
+// =====================================================================
+// C API
+// =====================================================================
+
+extern "C" void simint_init(void)
+{
+    init_tables();
+}
+
+extern "C" void simint_finalize(void)
+{
+    Workspace & w = workspace();
+    w.dpair.release();
+    w.dout.release();
+    w.dkord.release();
+    w.hstage.release();
+    w.hout.release();
+    if(w.stream)
+    {
+        cudaStreamDestroy(w.stream);
+        w.stream = nullptr;
+    }
+}
+
+extern "C" int simint_b200_set_ordering(int o)
+{
+    if(o != SIMINT_B200_ORDERING_PSI4 && o != SIMINT_B200_ORDERING_GAMESS)
+        return SIMINT_B200_ERR_ARG;
+    g_ordering = o;
+    return 0;
+}
+
+extern "C" int simint_b200_get_ordering(void) { return g_ordering; }
+
+extern "C" int simint_b200_set_precision(int mode, double gate)
+{
+    if(mode != SIMINT_B200_PREC_FP64 && mode != SIMINT_B200_PREC_MIXED)
+        return SIMINT_B200_ERR_ARG;
+    g_precision = mode;
+    g_gate = gate;
+    return 0;
+}
+
+extern "C" int simint_b200_get_precision(void) { return g_precision; }
+
+extern "C" const char * simint_b200_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" long long simint_b200_launch_count(void) { return t_launches; }
+
+extern "C" size_t simint_eri_worksize(int derorder, int maxam)
+{
+    return simint_ostei_worksize(derorder, maxam);
+}
+
+extern "C" size_t simint_eri_workmem(int derorder, int maxam)
+{
+    return simint_ostei_workmem(derorder, maxam);
+}
+
+namespace sb200 {
+
+// Launch the kernel of class req for the prepared arguments a (P, Q,
+// tasks or kord, ntask, check, tol2, out, nout filled by the caller).
+int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
+                 cudaStream_t stream)
+{
+    for(int k = 0; k < 4; k++)
+        if(req[k] < 0 || req[k] > SIMINT_OSTEI_MAXAM)
+        {
+            set_error("angular momentum outside 0..SIMINT_OSTEI_MAXAM");
+            return SIMINT_B200_ERR_CLASS;
+        }
+    if(a.ntask == 0)
+        return 0;
+    const UniqueMap u = unique_of(req);
+    a.swapB = u.swapB; a.swapK = u.swapK; a.pq = u.pq;
+    a.boys = boys_table();
+    if(deriv == 0)
+    {
+        const ClassKernels * k = find_kernels(u);
+        if(k)
+        {
+            a.oidx = oidx_table(req, u, ordering());
+            if(!a.oidx)
+            {
+                set_error("cannot allocate output index table");
+                return SIMINT_B200_ERR_CUDA;
+            }
+            const int threads = 128;
+            const long long blocks = (a.ntask + threads - 1) / threads;
+            KernFn fn = k->fn[mode][prec == SIMINT_B200_PREC_MIXED ? 1 : 0];
+            fn<<<(unsigned)blocks, threads, 0, stream>>>(a);
+            count_launch(1);
+            return 0;
+        }
+    }
+    return launch_generic(a, req, u, deriv, mode, stream);
+}
+
+// Run one P x Q rectangle on the device.  dP/dQ already hold packed pair
+// data; writes nout doubles per shell quartet to dout.
+int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
+                     const simint_multi_shellpair * Q, const PairSetDev & dQ,
+                     const int * dkord, double screen_tol, int deriv, int prec, double gatev,
+                     double * dout, cudaStream_t stream)
+{
+    const int req[4] = {P->am1, P->am2, Q->am1, Q->am2};
+    const int nc = ncart(req[0]) * ncart(req[1]) * ncart(req[2]) * ncart(req[3]);
+    KernArgs a;
+    memset(&a, 0, sizeof(a));
+    a.P = dP;
+    a.Q = dQ;
+    a.kord = dkord;
+    a.ntask = (long long)P->nshell12_clip * Q->nshell12_clip;
+    a.nQ = Q->nshell12_clip;
+    a.check = (screen_tol > 0.0) && P->screen && Q->screen;
+    a.tol2 = screen_tol * screen_tol;
+    a.gate = (prec == SIMINT_B200_PREC_MIXED) ? gatev : 0.0;
+    a.out = dout;
+    a.nout = nc * (deriv ? 12 : 1);
+    return launch_class(a, req, deriv, 0, prec, stream);
+}
+
+} // namespace sb200
+
+extern "C" int simint_compute_eri_deriv(int deriv,
+                                        struct simint_multi_shellpair const * P,
+                                        struct simint_multi_shellpair const * Q,
+                                        double screen_tol, double * work, double * integrals)
+{
+    (void)work;
+    if(!P || !Q || !integrals || deriv < 0 || deriv > SIMINT_OSTEI_MAXDER)
+    {
+        set_error("bad argument to simint_compute_eri_deriv");
+        return SIMINT_B200_ERR_ARG;
+    }
+    // pair-level early exit (ostei.c:16-19)
+    const double tol2 = screen_tol * screen_tol;
+    if(screen_tol > 0.0 && (P->screen_max * Q->screen_max) < tol2)
+        return -1;
+    init_tables();
+    if(ensure_device() < 0)
+        return SIMINT_B200_ERR_NODEVICE;
+    Workspace & w = workspace();
+    if(!w.stream && cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking) != cudaSuccess)
+    {
+        set_error("cudaStreamCreate failed");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    const long long nquart = (long long)P->nshell12_clip * Q->nshell12_clip;
+    if(nquart == 0)
+        return 0;
+    PackedLayout LP, LQ;
+    const size_t szP = (pack_pairs(P, nullptr, LP) + 255) & ~(size_t)255;
+    const size_t szQ = (pack_pairs(Q, nullptr, LQ) + 255) & ~(size_t)255;
+    // ket order: by primitive count (descending), stable
+    std::vector<int> kord(Q->nshell12_clip);
+    for(int k = 0; k < Q->nshell12_clip; k++) kord[k] = k;
+    std::stable_sort(kord.begin(), kord.end(), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+    const size_t szK = (kord.size() * sizeof(int) + 255) & ~(size_t)255;
+    if(!w.hstage.reserve(szP + szQ + szK) || !w.dpair.reserve(szP + szQ + szK))
+    {
+        set_error("out of memory for pair data");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    char * h = (char *)w.hstage.ptr;
+    pack_pairs(P, h, LP);
+    pack_pairs(Q, h + szP, LQ);
+    memcpy(h + szP + szQ, kord.data(), kord.size() * sizeof(int));
+    char * d = (char *)w.dpair.ptr;
+    cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
+    const PairSetDev dP = device_view(d, LP, P->screen_max);
+    const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
+    const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);
+    const size_t outbytes = (size_t)nquart * nc * sizeof(double);
+    if(!w.dout.reserve(outbytes))
+    {
+        set_error("out of device memory for the output");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    int r = launch_rectangle(P, dP, Q, dQ, (const int *)(d + szP + szQ), screen_tol, deriv,
+                             precision(), gate(), (double *)w.dout.ptr, w.stream);
+    if(r < 0)
+        return r;
+    cudaMemcpyAsync(integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost, w.stream);
+    cudaError_t e = cudaStreamSynchronize(w.stream);
+    if(e == cudaSuccess)
+        e = cudaGetLastError();
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    return (int)nquart;
+}
+
+extern "C" int simint_compute_eri(struct simint_multi_shellpair const * P,
+                                  struct simint_multi_shellpair const * Q,
+                                  double screen_tol, double * work, double * integrals)
+{
+    return simint_compute_eri_deriv(0, P, Q, screen_tol, work, integrals);
+}

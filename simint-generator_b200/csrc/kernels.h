@@ -1,0 +1,24 @@
+// Registry of the generated per-class kernels.
+#pragma once
+#include <vector>
+#include "ostei_device.cuh"
+
+typedef void (*KernFn)(const KernArgs);
+
+struct ClassKernels
+{
+    int am[4];           // unique class (a b | c d)
+    int L;               // a+b+c+d
+    int ntop;            // contracted top quartets
+    int vrr_flops;       // per primitive quartet (minimal plan)
+    int hrr_flops;       // per shell quartet
+    KernFn fn[2][2];     // [mode: 0 rectangle, 1 task list][prec: 0 FP64, 1 mixed]
+};
+
+struct KernelTable
+{
+    std::vector<ClassKernels> list;
+    void add(const ClassKernels & k) { list.push_back(k); }
+};
+
+void simint_b200_register_generated(KernelTable & t);

@@ -1,0 +1,84 @@
+// Internal declarations shared by the host runtime files.
+#pragma once
+
+#include <array>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "simint/simint.h"
+#include "ostei_device.cuh"
+#include "kernels.h"
+
+namespace sb200 {
+
+struct UniqueMap
+{
+    int am[4];
+    int swapB, swapK, pq;
+};
+
+struct DevBuf
+{
+    void * ptr = nullptr;
+    size_t cap = 0;
+    bool reserve(size_t n);
+    void release();
+};
+
+struct HostBuf
+{
+    void * ptr = nullptr;
+    size_t cap = 0;
+    bool reserve(size_t n);
+    void release();
+};
+
+struct Workspace
+{
+    cudaStream_t stream = nullptr;
+    DevBuf dpair, dout, dkord, dscratch;
+    HostBuf hstage, hout;
+    ~Workspace();
+};
+
+struct PackedLayout
+{
+    int npad = 0, npair = 0;
+    size_t off_rec = 0, off_start = 0, off_nprim = 0, off_AB = 0;
+};
+
+void set_error(const std::string & s);
+void count_launch(long long n);
+int ensure_device();
+const double * boys_table();
+void init_tables();
+int ordering();
+int precision();
+double gate();
+Workspace & workspace();
+UniqueMap unique_of(const int am[4]);
+const ClassKernels * find_kernels(const UniqueMap & u);
+int cart_index(int i, int j, int k, int ordering);
+void carts(int l, std::vector<std::array<int, 3>> & out);
+void pair_starts(const simint_multi_shellpair * P, std::vector<int> & start, int & npad);
+size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L);
+PairSetDev device_view(const char * base, const PackedLayout & L, double screen_max);
+const unsigned short * oidx_table(const int req[4], const UniqueMap & u, int ord);
+
+int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
+                     const simint_multi_shellpair * Q, const PairSetDev & dQ,
+                     const int * dkord, double screen_tol, int deriv, int prec, double gatev,
+                     double * dout, cudaStream_t stream);
+
+int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
+                 cudaStream_t stream);
+
+// Generic (table-driven, dense) kernel for classes without a straight-line
+// kernel and for deriv=1.  Everything in a except the role swaps is filled.
+int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deriv, int mode,
+                   cudaStream_t stream);
+
+int ncart_of(int l);
+
+} // namespace sb200

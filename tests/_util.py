@@ -1,0 +1,46 @@
+"""Shared helpers for the tests (parity comparisons and shell sets)."""
+import ctypes as C
+import itertools
+
+import numpy as np
+
+from simint_b200.capi import ShellSet, SimintMultiShellpair, ShellP
+from simint_b200.workloads import random_shells
+
+NC = lambda l: (l + 1) * (l + 2) // 2
+
+# Parity bar of the FP64 path against the CPU oracle, per element:
+# |d| <= 1e-13, or |ref| > 1e-15 and |d|/|ref| <= 1e-11.
+ABS_TOL = 1e-13
+REL_TOL = 1e-11
+
+
+def parity_bad(calc, ref, abs_tol=ABS_TOL, rel_tol=REL_TOL):
+    """Indices failing the abs-or-rel bar."""
+    d = np.abs(calc - ref)
+    rel = np.where(np.abs(ref) > 1e-15, d / np.maximum(np.abs(ref), 1e-300), np.inf)
+    bad = (d > abs_tol) & ~(rel <= rel_tol)
+    return np.nonzero(bad)[0], d.max() if d.size else 0.0
+
+
+def class_shells(rng, am, nsh=(2, 1, 2, 1), nprim=(1, 3), alpha=(0.1, 20.0), box=3.0):
+    ams = [am[0]] * nsh[0] + [am[1]] * nsh[1] + [am[2]] * nsh[2] + [am[3]] * nsh[3]
+    shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box)
+    idx = np.cumsum([0] + list(nsh))
+    grp = [list(range(idx[k], idx[k + 1])) for k in range(4)]
+    return shells, grp
+
+
+def oracle_pairs(orc, S, pairs, screen=0):
+    P = SimintMultiShellpair()
+    arr = S.pair_list(pairs)
+    orc.oracle_create_pair(len(pairs), C.cast(arr, ShellP), C.byref(P), screen)
+    return P
+
+
+def oracle_eri(orc, P, Q, tol=0.0, deriv=0, ordering=0):
+    n = P.nshell12_clip * Q.nshell12_clip * NC(P.am1) * NC(P.am2) * NC(Q.am1) * NC(Q.am2)
+    out = np.zeros(n * (12 if deriv else 1))
+    r = orc.oracle_compute_eri(C.byref(P), C.byref(Q), tol, deriv, ordering,
+                               out.ctypes.data_as(C.POINTER(C.c_double)))
+    return r, out
