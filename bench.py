@@ -1,0 +1,407 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 Simint engine (one JSON line on stdout).
+
+Workload ("cfg2"): 500 seeded synthetic shells, s:p:d:f = 200:150:100:50,
+1-8 primitives, exponents log-uniform in [0.05, 5e4], 120 pseudo-atoms in a
+20 bohr cube; every shell quartet surviving the shell-pair Schwarz test
+Q_ab*Q_cd >= 1e-14, primitive screening at the same tolerance.  The full
+sweep (1.9e9 quartets, 1e11 primitive quartets) is far beyond one step, so a
+step is one pass over a proportional stratified subsample of it: every
+`--stride`-th bra-pair row of every AM class (the class mix of the whole
+sweep is kept).  Metric: evaluated primitive quartets per second.  `value`
+is the mixed-precision batched path (FP32 VRR where the Schwarz bound allows,
+FP64 elsewhere); the FP64 path is reported beside it.
+
+Arms:
+  default            B200 sweep (device-resident inputs; CUDA-graph replay),
+                     plus e2e through simint_compute_eri with host buffers and
+                     the CPU oracle timed on the host cores (cpu_baseline).
+  --impl reference   the CPU restatement of the reference algorithm (the
+                     oracle; the reference's own kernels exist only as its
+                     code generator's output) on the host cores, over the
+                     same simint_compute_eri calls as e2e.
+
+N > 1 (torchrun): each rank sweeps a disjoint shard (row offset = rank), no
+collective on the data path; ranks meet at barriers around the timed region
+and the max device time is taken.
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "simint-generator_b200"))
+
+TOL = 1e-14
+MAX_AM = 3
+SEED = 2024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--stride", type=int, default=2000,
+                    help="keep every stride-th bra-pair row of each class")
+    ap.add_argument("--e2e-stride", type=int, default=40000)
+    ap.add_argument("--gate", type=float, default=None,
+                    help="mixed-precision Schwarz-bound gate (default: from the error model)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# helpers
+# ----------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def workload_shells(lib):
+    from simint_b200.capi import ShellSet
+    from simint_b200.workloads import config_shells
+    shells = config_shells("cfg2")
+    S = ShellSet(shells)
+    lib.simint_normalize_shells(S.n, S.ptr(0))
+    return S
+
+
+def pack_bytes(P):
+    """Bytes simint_compute_eri uploads for one pair set (packed records)."""
+    from simint_b200.capi import padded_nprim
+    a256 = lambda n: (n + 255) & ~255
+    return a256(padded_nprim(P) * 16 * 8 + 2 * a256(P.nshell12 * 4) + 24 * P.nshell12)
+
+
+def e2e_rows(sb, lib, S, B, stride, rank=0):
+    """Host pair objects (P = one bra pair, Q = its screened ket list) for a
+    proportional sample of the sweep's rows."""
+    rows = []
+    for k, c in enumerate(B.classes()):
+        rr = B.rows(k)
+        for r in range(rank % stride, len(rr), stride):
+            first, n = rr[r]
+            q0 = B.quartet(k, first)
+            kets = [B.quartet(k, first + i)[2:] for i in range(n)]
+            P = sb.make_pairs(lib, S, [q0[:2]], sb.SIMINT_SCREEN_SCHWARZ)
+            Q = sb.make_pairs(lib, S, kets, sb.SIMINT_SCREEN_SCHWARZ)
+            rows.append((c["am"], P, Q))
+    return rows
+
+
+def flops_of_class(am, nprimq, nquart):
+    """Algorithmic FLOPs (minimal recurrence plan; FMA = 2): per primitive
+    quartet set-up + Boys + VRR + contraction adds + 3 div + 1 sqrt, per
+    shell quartet the HRR."""
+    from simint_b200.gen.emit import unique_class
+    from simint_b200.gen.plan import class_plan
+    u = unique_class(am)[0]
+    p = class_plan(*u)
+    L = p.L
+    boys = 16 * (L + 1) if L < 4 else 16 + 3 * L + 20
+    setup = 30 + (L + 1)
+    per_prim = setup + boys + p.vrr_flops() + p.ntop() + 4
+    return nprimq * per_prim + nquart * p.hrr_flops()
+
+
+# ----------------------------------------------------------------------------
+# arms
+# ----------------------------------------------------------------------------
+
+def cpu_bench(rows, budget_s, threads):
+    """(primq/s, seconds, primq, nrows) of the oracle over a row sample that
+    takes about budget_s on `threads` host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import load_oracle
+    from simint_b200.capi import PairP
+    orc = load_oracle()
+
+    def run(idx):
+        PP = (PairP * len(idx))(*[C.pointer(rows[i][1]) for i in idx])
+        QQ = (PairP * len(idx))(*[C.pointer(rows[i][2]) for i in idx])
+        npq = C.c_longlong()
+        cs = C.c_double()
+        t = orc.oracle_bench_rows(len(idx), PP, QQ, TOL, threads, C.byref(npq), C.byref(cs))
+        return t, npq.value
+
+    # interleave classes so any prefix keeps the class mix
+    idx = list(range(0, len(rows), max(1, len(rows) // 64)))[:64]
+    t, n = run(idx)
+    scale = budget_s / max(t, 1e-3)
+    take = max(1, min(len(rows), int(len(idx) * scale)))
+    step = max(1, len(rows) // take)
+    idx = list(range(0, len(rows), step))[:take]
+    t, n = run(idx)
+    return n / t, t, n, len(idx)
+
+
+def run_reference(args):
+    import simint_b200 as sb
+    lib = sb.load()
+    lib.simint_init()
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    S = workload_shells(lib)
+    B = sb.Basis(S, TOL, MAX_AM, lib)
+    B.subsample_stride(args.stride, 0)
+    rows = e2e_rows(sb, lib, S, B, max(1, args.e2e_stride // args.stride))
+    threads = os.cpu_count() or 1
+    vals = []
+    for _ in range(args.warmup):
+        cpu_bench(rows, args.cpu_seconds / 4, threads)
+    for _ in range(args.steps):
+        rate, t, n, nr = cpu_bench(rows, args.cpu_seconds, threads)
+        vals.append((rate, t, n, nr))
+    rate = statistics.median(v[0] for v in vals)
+    t = statistics.median(v[1] for v in vals)
+    out = {
+        "impl": "reference", "metric": "primitive quartets/s (cfg2 l<=3 sweep sample, screen_tol 1e-14)",
+        "value": rate, "unit": "primitive quartets/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 shells)",
+        "config": {"workload": "cfg2: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, 120 atoms, "
+                               "Schwarz 1e-14; simint_compute_eri rows (1 bra pair x screened kets)",
+                   "sample_rows": vals[-1][3], "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": rate, "unit": "primitive quartets/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d simint_compute_eri-shaped rows of the cfg2 sweep sample, %.3g primitive quartets"
+                                   % (vals[-1][3], vals[-1][2])},
+        "e2e": {"value": rate, "unit": "primitive quartets/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def run_b200(args):
+    import torch
+    import simint_b200 as sb
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    lib = sb.load()
+    lib.simint_init()
+    S = workload_shells(lib)
+    t0 = time.time()
+    B = sb.Basis(S, TOL, MAX_AM, lib)
+    nfull = sum(B.class_full(k) for k in range(len(B.classes())))
+    B.subsample_stride(args.stride * world, rank * args.stride)
+    npq = B.count_primq()
+    classes = B.classes()
+    setup_s = time.time() - t0
+    stream = torch.cuda.current_stream()
+    cap = max(1, min(B.output_size, (4 << 30) // 8))
+    out = torch.empty(cap, dtype=torch.float64, device="cuda")
+    flush = torch.empty((256 << 20) // 4, dtype=torch.float32, device="cuda")   # > L2 (126 MB)
+    peak64 = sb.fma_peak(False, lib)
+    peak32 = sb.fma_peak(True, lib)
+    gate = args.gate if args.gate is not None else 1e-6
+
+    def timed(prec):
+        lib.simint_b200_set_precision(prec, gate)
+        nl = 0
+        for _ in range(args.warmup):
+            nl = B.compute(prec, out.data_ptr(), cap, stream.cuda_stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                nl = B.compute(prec, out.data_ptr(), cap, stream.cuda_stream)
+                e1.record(stream)
+                ms.append((e0, e1))
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        tot = sum(a.elapsed_time(b) for a, b in ms)
+        if dist:
+            tt = torch.tensor([tot], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            tot = float(tt.item())
+        return tot / args.steps, nl, clk.summary()
+
+    ms64, nl64, clk64 = timed(sb.FP64)
+    sums64 = B.checksums()
+    msmx, nlmx, clkmx = timed(sb.MIXED)
+    sumsmx = B.checksums()
+    lib.simint_b200_set_precision(sb.FP64, 0.0)
+    ct64 = B.class_times(sb.FP64, out.data_ptr(), cap, stream.cuda_stream)
+    lib.simint_b200_set_precision(sb.MIXED, gate)
+    ctmx = B.class_times(sb.MIXED, out.data_ptr(), cap, stream.cuda_stream)
+    lib.simint_b200_set_precision(sb.FP64, 0.0)
+    total_npq = npq
+    if dist:
+        tt = torch.tensor([float(npq)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt)
+        total_npq = float(tt.item())
+    value = total_npq / (msmx / 1e3)
+    value64 = total_npq / (ms64 / 1e3)
+
+    per_class = []
+    for k, c in enumerate(classes):
+        fl = flops_of_class(c["am"], c["nprimq"], c["nquart"])
+        per_class.append({"am": "".join("spdfg"[x] for x in c["am"]), "quartets": c["nquart"],
+                          "primq": c["nprimq"], "ms_fp64": round(ct64[k], 4), "ms_mixed": round(ctmx[k], 4),
+                          "primq_s_fp64": c["nprimq"] / max(ct64[k], 1e-9) * 1e3,
+                          "primq_s_mixed": c["nprimq"] / max(ctmx[k], 1e-9) * 1e3,
+                          "fp64_tflops": fl / max(ct64[k], 1e-9) / 1e9,
+                          "checksum_fp64": float(sums64[k, 0]), "checksum_mixed": float(sumsmx[k, 0]),
+                          "abssum_fp64": float(sums64[k, 1])})
+    dom = max(range(len(classes)), key=lambda k: ctmx[k])
+    dc = classes[dom]
+    dom_fl = flops_of_class(dc["am"], dc["nprimq"], dc["nquart"])
+    achieved = dom_fl / (ctmx[dom] / 1e3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("".join("spdfg"[x] for x in dc["am"]))
+        except Exception:
+            traffic = None
+
+    # e2e through the reference-facing C ABI, host buffers
+    e2e = None
+    cpu = None
+    if rank == 0:
+        rows = e2e_rows(sb, lib, S, B, max(1, args.e2e_stride // args.stride))
+        lib.simint_b200_set_precision(sb.MIXED, gate)
+        npq_e2e = sum(sb.count_primq(P, Q, TOL, lib) for _, P, Q in rows)
+        h2d = sum(pack_bytes(P) + pack_bytes(Q) for _, P, Q in rows)
+        bufs = [np.empty(P.nshell12_clip * Q.nshell12_clip * sb.ncart(P.am1) * sb.ncart(P.am2)
+                         * sb.ncart(Q.am1) * sb.ncart(Q.am2)) for _, P, Q in rows]
+        d2h = sum(b.nbytes for b in bufs)
+        dp = C.POINTER(C.c_double)
+        for _ in range(max(1, args.warmup)):
+            for (am, P, Q), buf in zip(rows, bufs):
+                lib.simint_compute_eri(C.byref(P), C.byref(Q), TOL, None, buf.ctypes.data_as(dp))
+        times = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            for (am, P, Q), buf in zip(rows, bufs):
+                r = lib.simint_compute_eri(C.byref(P), C.byref(Q), TOL, None, buf.ctypes.data_as(dp))
+                if r < -1:
+                    raise RuntimeError(sb.last_error())
+            times.append(time.perf_counter() - t)
+        lib.simint_b200_set_precision(sb.FP64, 0.0)
+        e2e = {"value": npq_e2e / statistics.median(times), "unit": "primitive quartets/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "calls_per_step": len(rows), "primq_per_step": int(npq_e2e)}
+        if not args.no_cpu:
+            threads = os.cpu_count() or 1
+            rate, t, n, nr = cpu_bench(rows, args.cpu_seconds, threads)
+            cpu = {"value": rate, "unit": "primitive quartets/s", "cores": threads, "kind": "port",
+                   "sample": "%d of the e2e simint_compute_eri rows (%.3g primitive quartets, %.1f s)"
+                             % (nr, n, t)}
+
+    if rank == 0:
+        launches = nlmx // 2 * args.steps      # ERI kernels (checksum kernels excluded)
+        res = {
+            "metric": "primitive quartets/s, mixed-precision batched sweep (cfg2 l<=3, screen 1e-14)",
+            "value": value, "unit": "primitive quartets/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the Schwarz gate)",
+            "data": "synthetic (seeded cfg2 shells, PCG64 seed 2024)",
+            "config": {"workload": "cfg2 sweep sample: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, "
+                                   "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14; every %d-th bra "
+                                   "row of every class" % (args.stride * world),
+                       "quartets_per_step": int(sum(c["nquart"] for c in classes)),
+                       "primq_per_step": int(total_npq), "full_sweep_quartets": int(nfull),
+                       "gate": gate, "l2": "256 MB flush before every timed step",
+                       "parallelism": "dp%d (disjoint row shards)" % world, "setup_s": round(setup_s, 1)},
+            "fp64": {"value": value64, "ms_per_step": ms64},
+            "roofline": {"bound": "fp64", "kernel": "class " + "".join("spdfg"[x] for x in dc["am"]),
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                         "frac": achieved / peak64 if peak64 > 0 else None, "traffic": traffic,
+                         "peak_source": "measured FMA-chain probe (simint_b200_fma_peak)",
+                         "fp32_peak": peak32},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clkmx, "clocks_fp64": clk64, "per_class": per_class,
+        }
+        print(json.dumps(res))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -65,18 +65,85 @@ simint_b200_basis * simint_b200_basis_create(int nshell, struct simint_shell con
                                              double screen_tol, int max_am);
 void simint_b200_basis_free(simint_b200_basis * b);
 
+/* Keep a deterministic stratified subsample of every class: bra-pair rows
+ * are taken with a constant stride chosen so a class keeps about
+ * max_quartets quartets (classes already smaller keep everything).  Used to
+ * bound benchmark steps on very large sweeps; the full-sweep quartet counts
+ * stay available through simint_b200_basis_class_full. */
+int simint_b200_basis_subsample(simint_b200_basis * b, long long max_quartets);
+
+/* Quartets of class k before subsampling. */
+long long simint_b200_basis_class_full(simint_b200_basis const * b, int k);
+
+/* Count the primitive quartets that survive primitive screening in the
+ * current task lists (one device pass); returns the total. */
+long long simint_b200_basis_count_primq(simint_b200_basis * b);
+
 /* Quartet and primitive-quartet counts of the sweep (after screening). */
 long long simint_b200_basis_nquartets(simint_b200_basis const * b);
 long long simint_b200_basis_nprimquartets(simint_b200_basis const * b);
 /* Number of doubles the full output of the sweep occupies. */
 long long simint_b200_basis_output_size(simint_b200_basis const * b);
 
-/* Run the sweep on `stream` (cudaStream_t, may be NULL) writing all
- * integrals to device memory `dev_out` (simint_b200_basis_output_size
- * doubles), class after class, quartets in the order of
- * simint_b200_basis_tasks.  prec selects FP64 or mixed.  Returns the number
- * of kernel launches, or a negative error code. */
-int simint_b200_basis_compute(simint_b200_basis * b, int prec, double * dev_out, void * stream);
+/* Run the sweep on `stream` (cudaStream_t, may be NULL).  Integrals are
+ * written to device memory dev_out of dev_out_doubles doubles.  When that
+ * holds the whole sweep (simint_b200_basis_output_size), class k starts at
+ * its class offset and quartet q of the class at offset + q*nout; otherwise
+ * the sweep is streamed through dev_out in chunks (each chunk overwrites the
+ * previous one).  Either way per-class checksums are accumulated (see
+ * simint_b200_basis_checksums).  prec selects FP64 or mixed.  The launches
+ * are captured once into a CUDA graph per (prec, buffer) and replayed.
+ * Returns the number of kernel launches of one sweep, or a negative code. */
+int simint_b200_basis_compute(simint_b200_basis * b, int prec, double * dev_out,
+                              long long dev_out_doubles, void * stream);
+
+/* Number of AM classes in the sweep and their description: requested class
+ * am[4], quartets, evaluated primitive quartets (after the reference's
+ * primitive screening), doubles per quartet, offset of the class in a full
+ * output buffer. */
+int simint_b200_basis_nclass(simint_b200_basis const * b);
+int simint_b200_basis_class_info(simint_b200_basis const * b, int k, int am[4],
+                                 long long * nquart, long long * nprimq,
+                                 int * nout, long long * offset);
+
+/* The (bra pair, ket pair) shells of quartet q of class k:
+ * shells[0..3] = indices into the shell array given to basis_create. */
+int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, int shells[4]);
+
+/* Per-class checksums of the last compute: sums[2k] = sum of values,
+ * sums[2k+1] = sum of absolute values.  Waits for the stream. */
+int simint_b200_basis_checksums(simint_b200_basis * b, double * sums);
+
+/* Device time of each class in one (non-graph) sweep, milliseconds. */
+int simint_b200_basis_class_times(simint_b200_basis * b, int prec, double * dev_out,
+                                  long long dev_out_doubles, void * stream, float * ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Keep bra-pair rows offset, offset+stride, ... of every class (a
+ * proportional stratified subsample: the class mix of the full sweep is
+ * preserved; disjoint offsets give disjoint shards). */
+int simint_b200_basis_subsample_stride(simint_b200_basis * b, int stride, int offset);
+
+/* Rows of class k (one bra pair each) and the task range of row r. */
+int simint_b200_basis_nrows(simint_b200_basis const * b, int k);
+int simint_b200_basis_row(simint_b200_basis const * b, int k, int r, long long * first, long long * n);
+
+/* Primitive quartets simint_compute_eri(P, Q, screen_tol) evaluates: the
+ * reference's bra-primitive and 8-wide ket-vector screening applied to the
+ * host pair data (no device work). */
+long long simint_b200_count_primq(struct simint_multi_shellpair const * P,
+                                  struct simint_multi_shellpair const * Q, double screen_tol);
+
+/* Measured FMA throughput of the current device in TFLOP/s: FP64 (fp32 = 0)
+ * or FP32 (fp32 = 1).  Used as the roofline denominator. */
+double simint_b200_fma_peak(int fp32);
 
 #ifdef __cplusplus
 }

@@ -39,6 +39,9 @@ def load_oracle():
     lib.oracle_bench_omp.argtypes = [C.c_int, PairP, PairP, C.c_double, C.c_int, C.c_int,
                                      C.c_int, _dp]
     lib.oracle_bench_omp.restype = C.c_double
+    lib.oracle_bench_rows.argtypes = [C.c_int, C.POINTER(PairP), C.POINTER(PairP), C.c_double,
+                                      C.c_int, C.POINTER(C.c_longlong), _dp]
+    lib.oracle_bench_rows.restype = C.c_double
     return lib
 
 

@@ -38,6 +38,49 @@ __global__ void k_diag_max(const double * __restrict__ ints, int n1, int n2, lon
 
 namespace sb200 {
 
+// max over the diagonal Cartesians of (ab|ab) for every shell pair k < n of
+// a packed pair set, written to dmax[k] (device).  Runs the class kernel on
+// the task list (k, k) in chunks of at most 512 MiB of (ab|ab) blocks.
+int pair_diag_max(const PairSetDev & dP, int am1, int am2, int n, double * dmax, cudaStream_t stream)
+{
+    Workspace & w = workspace();
+    const int n1 = ncart_of(am1), n2 = ncart_of(am2);
+    const long long nc = (long long)n1 * n2 * n1 * n2;
+    const long long chunk = std::max<long long>(1, std::min<long long>(n, (512ll << 20) / (nc * 8)));
+    std::vector<int2> ht(chunk);
+    if(!w.dkord.reserve((size_t)chunk * sizeof(int2)) || !w.dout.reserve((size_t)chunk * nc * sizeof(double)))
+    {
+        set_error("out of device memory in pair_diag_max");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    int2 * dtask = (int2 *)w.dkord.ptr;
+    for(long long c0 = 0; c0 < n; c0 += chunk)
+    {
+        const long long cn = std::min<long long>(chunk, n - c0);
+        cudaStreamSynchronize(stream);       // host task staging is reused
+        for(long long k = 0; k < cn; k++)
+            ht[k] = make_int2((int)(c0 + k), (int)(c0 + k));
+        cudaMemcpyAsync(dtask, ht.data(), cn * sizeof(int2), cudaMemcpyHostToDevice, stream);
+        KernArgs a;
+        memset(&a, 0, sizeof(a));
+        a.P = dP; a.Q = dP;
+        a.tasks = dtask;
+        a.ntask = cn;
+        a.out = (double *)w.dout.ptr;
+        a.nout = (int)nc;
+        const int req[4] = {am1, am2, am1, am2};
+        // the diagonal does not depend on the Cartesian ordering
+        int rc = launch_class(a, req, 0, 1, SIMINT_B200_PREC_FP64, stream);
+        if(rc != 0)
+            return rc;
+        k_diag_max<<<(unsigned)((cn + 127) / 128), 128, 0, stream>>>(
+            (double *)w.dout.ptr, n1, n2, cn, nc, dmax + c0);
+        count_launch(1);
+    }
+    cudaStreamSynchronize(stream);
+    return 0;
+}
+
 int prim_schwarz_batch(int npair, const simint_shell * AB, double * out)
 {
     init_tables();
@@ -99,15 +142,8 @@ int prim_schwarz_batch(int npair, const simint_shell * AB, double * out)
     }
     PackedLayout LP;
     const size_t szP = (pack_pairs(&PP, nullptr, LP) + 255) & ~(size_t)255;
-    const int am1 = AB[0].am, am2 = AB[1].am;
-    const int n1 = ncart_of(am1), n2 = ncart_of(am2);
-    const long long nc = (long long)n1 * n2 * n1 * n2;
-    // chunk so the (ab|ab) blocks stay under 512 MiB
-    const long long chunk = std::max<long long>(1, std::min<long long>(n, (512ll << 20) / (nc * 8)));
-    const size_t szT = ((size_t)chunk * sizeof(int2) + 255) & ~(size_t)255;
     const size_t szM = ((size_t)n * sizeof(double) + 255) & ~(size_t)255;
-    if(!w.hstage.reserve(szP + szT) || !w.dpair.reserve(szP + szT + szM) ||
-       !w.dout.reserve((size_t)chunk * nc * sizeof(double)))
+    if(!w.hstage.reserve(szP) || !w.dpair.reserve(szP + szM))
     {
         simint_free_multi_shellpair(&PP);
         set_error("out of memory in Schwarz screening");
@@ -118,34 +154,8 @@ int prim_schwarz_batch(int npair, const simint_shell * AB, double * out)
     pack_pairs(&PP, h, LP);
     cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream);
     const PairSetDev dP = device_view(d, LP, PP.screen_max);
-    int2 * dtask = (int2 *)(d + szP);
-    double * dmax = (double *)(d + szP + szT);
-    int rc = 0;
-    for(long long c0 = 0; c0 < n && rc == 0; c0 += chunk)
-    {
-        const long long cn = std::min<long long>(chunk, n - c0);
-        int2 * ht = (int2 *)(h + szP);
-        cudaStreamSynchronize(w.stream);       // staging reuse
-        for(long long k = 0; k < cn; k++)
-            ht[k] = make_int2((int)(c0 + k), (int)(c0 + k));
-        cudaMemcpyAsync(dtask, ht, cn * sizeof(int2), cudaMemcpyHostToDevice, w.stream);
-        KernArgs a;
-        memset(&a, 0, sizeof(a));
-        a.P = dP; a.Q = dP;
-        a.tasks = dtask;
-        a.ntask = cn;
-        a.out = (double *)w.dout.ptr;
-        a.nout = (int)nc;
-        const int req[4] = {am1, am2, am1, am2};
-        // the diagonal does not depend on the Cartesian ordering
-        rc = launch_class(a, req, 0, 1, SIMINT_B200_PREC_FP64, w.stream);
-        if(rc == 0)
-        {
-            k_diag_max<<<(unsigned)((cn + 127) / 128), 128, 0, w.stream>>>(
-                (double *)w.dout.ptr, n1, n2, cn, nc, dmax + c0);
-            count_launch(1);
-        }
-    }
+    double * dmax = (double *)(d + szP);
+    int rc = pair_diag_max(dP, AB[0].am, AB[1].am, n, dmax, w.stream);
     std::vector<double> mx(n);
     if(rc == 0)
     {

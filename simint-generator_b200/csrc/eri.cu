@@ -479,6 +479,8 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
             return 0;
         }
     }
+    if(coop_supported(req, deriv))
+        return launch_coop(a, req, deriv, mode, stream);
     return launch_generic(a, req, u, deriv, mode, stream);
 }
 
@@ -584,4 +586,33 @@ extern "C" int simint_compute_eri(struct simint_multi_shellpair const * P,
                                   double screen_tol, double * work, double * integrals)
 {
     return simint_compute_eri_deriv(0, P, Q, screen_tol, work, integrals);
+}
+
+extern "C" long long simint_b200_count_primq(struct simint_multi_shellpair const * P,
+                                             struct simint_multi_shellpair const * Q, double screen_tol)
+{
+    const double tol2 = screen_tol * screen_tol;
+    if(screen_tol > 0.0 && P->screen_max * Q->screen_max < tol2)
+        return 0;
+    const bool check = screen_tol > 0.0 && P->screen && Q->screen;
+    std::vector<int> ps, qs;
+    int npP = 0, npQ = 0;
+    pair_starts(P, ps, npP);
+    pair_starts(Q, qs, npQ);
+    std::vector<double> vmax((npQ + 7) / 8, 0.0);
+    if(check)
+        for(int j = 0; j < npQ; j++)
+            vmax[j / 8] = std::max(vmax[j / 8], Q->screen[j]);
+    long long n = 0;
+    for(int ab = 0; ab < P->nshell12_clip; ab++)
+        for(int i = ps[ab]; i < ps[ab] + P->nprim12[ab]; i++)
+        {
+            if(check && P->screen[i] * Q->screen_max < tol2)
+                continue;
+            for(int cd = 0; cd < Q->nshell12_clip; cd++)
+                for(int j = qs[cd]; j < qs[cd] + Q->nprim12[cd]; j++)
+                    if(!check || P->screen[i] * vmax[j / 8] >= tol2)
+                        n++;
+        }
+    return n;
 }

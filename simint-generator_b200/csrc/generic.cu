@@ -511,8 +511,10 @@ int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deri
     const unsigned blocks = (unsigned)((nthr + threads - 1) / threads);
     if(mode == 0)
         k_generic<0><<<blocks, threads, 0, stream>>>(a, g, (double *)w.dscratch.ptr, nthr);
-    else
+    else if(mode == 1)
         k_generic<1><<<blocks, threads, 0, stream>>>(a, g, (double *)w.dscratch.ptr, nthr);
+    else
+        k_generic<2><<<blocks, threads, 0, stream>>>(a, g, (double *)w.dscratch.ptr, nthr);
     count_launch(1);
     return 0;
 }

@@ -12,7 +12,7 @@ struct ClassKernels
     int ntop;            // contracted top quartets
     int vrr_flops;       // per primitive quartet (minimal plan)
     int hrr_flops;       // per shell quartet
-    KernFn fn[2][2];     // [mode: 0 rectangle, 1 task list][prec: 0 FP64, 1 mixed]
+    KernFn fn[3][2];     // [mode: 0 rectangle, 1 task list, 2 screened sweep][prec: 0 FP64, 1 mixed]
 };
 
 struct KernelTable

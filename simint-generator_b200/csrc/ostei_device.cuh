@@ -45,6 +45,13 @@ struct KernArgs
     int nout;                 // doubles per shell quartet
     int * status;             // device status word (error flags)
     const double * boys;      // Boys tables (see SB_BOYS_LONGFAC_OFF)
+    // MODE 2 (screened sweep): bra pairs border[b], b < nb, each with the
+    // ket pairs korder[0 .. prefix[b+1]-prefix[b]); tasks task0.. of it
+    const long long * prefix;
+    const int * border;
+    const int * korder;
+    int nb;
+    long long task0;
 };
 
 struct QuartetCtx
@@ -185,21 +192,29 @@ __device__ __forceinline__ BraPrim load_bra_prim(const QuartetCtx & c, int i)
     return b;
 }
 
+// Screening test of ket primitive j against bra primitive bp (only called
+// when screening is on): the reference's 8-wide vector test, plus its
+// bra-level test when the requested bra set plays the ket role.
+__device__ __forceinline__ bool prim_survives(const QuartetCtx & c, const BraPrim & bp, int j)
+{
+    const double * r = c.kprim + (size_t)j * SB_REC;
+    const double ks = r[13], kv = r[14];
+    const double v = c.pq ? ks * bp.vecmax : bp.screen * kv;
+    if(v < c.tol2)
+        return false;
+    if(c.pq && ks * c.bscreen_max < c.tol2)
+        return false;
+    return true;
+}
+
 // Ket primitive j against bra primitive bp: screening, then the
 // per-primitive-quartet set-up of OSTEI_Writer.cpp:586-702.
 __device__ __forceinline__ bool prim_setup(const QuartetCtx & c, const BraPrim & bp, int j,
                                            PrimSetup & s)
 {
     const double * r = c.kprim + (size_t)j * SB_REC;
-    if(c.check)
-    {
-        const double ks = r[13], kv = r[14];
-        const double v = c.pq ? ks * bp.vecmax : bp.screen * kv;
-        if(v < c.tol2)
-            return false;
-        if(c.pq && ks * c.bscreen_max < c.tol2)
-            return false;
-    }
+    if(c.check && !prim_survives(c, bp, j))
+        return false;
     const double q = r[0];
     const double p = bp.alpha;
     const double sum = p + q;
@@ -284,12 +299,26 @@ __device__ __forceinline__ bool task_of(const KernArgs & a, long long t, int & i
         iQ = a.kord[t - (long long)iP * a.nQ];
         off = ((long long)iP * a.nQ + iQ) * a.nout;
     }
-    else
+    else if(MODE == 1)
     {
         const int2 tk = a.tasks[t];
         iP = tk.x;
         iQ = tk.y;
         off = a.outoff ? a.outoff[t] : t * (long long)a.nout;
+    }
+    else
+    {
+        // largest b with prefix[b] <= tg (binary search over nb+1 entries)
+        const long long tg = a.task0 + t;
+        int lo = 0, hi = a.nb;
+        while(hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if(__ldg(a.prefix + mid) <= tg) lo = mid; else hi = mid;
+        }
+        iP = __ldg(a.border + lo);
+        iQ = __ldg(a.korder + (int)(tg - __ldg(a.prefix + lo)));
+        off = t * (long long)a.nout;
     }
     return true;
 }

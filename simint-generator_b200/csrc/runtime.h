@@ -80,5 +80,8 @@ int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deri
                    cudaStream_t stream);
 
 int ncart_of(int l);
+bool coop_supported(const int am[4], int deriv);
+int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_t stream);
+int pair_diag_max(const PairSetDev & dP, int am1, int am2, int n, double * dmax, cudaStream_t stream);
 
 } // namespace sb200

@@ -1,0 +1,638 @@
+// Batched, device-resident ERI sweeps over a whole basis.
+//
+// The reference's callers express a sweep as many simint_compute_eri calls
+// (one bra pair against a ket list, skel/test/benchmark_eri.cpp:135-216, or
+// Psi4/GTFock integral loops).  Here a basis is uploaded once:
+//   * shell pairs (i >= j) are grouped into pair classes (la >= lb) and built
+//     with primitive Schwarz screening (values computed on the GPU),
+//   * every shell pair gets its Schwarz bound Q_ab = sqrt(max |(ab|ab)|)
+//     (simint_shellscreen_schwarz, shell_screen.c:48-83), also on the GPU,
+//   * pairs are sorted by Q_ab, so for each bra pair the surviving ket pairs
+//     (Q_ab Q_cd >= tol) are a prefix of the sorted ket list; a prefix-sum
+//     array over bra pairs is the whole task list of a quartet class
+//     (kernels decode task t by binary search: no explicit quartet list),
+//   * inside a quartet the reference's primitive screening applies with the
+//     same tolerance (pairs built with SIMINT_SCREEN_SCHWARZ).
+// A sweep launches one kernel per class (or per output chunk), adds a
+// checksum kernel per launch, and is captured into one CUDA graph.
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "simint/simint.h"
+#include "simint_b200.h"
+#include "runtime.h"
+
+using namespace sb200;
+
+namespace {
+
+struct PairClass
+{
+    int la = 0, lb = 0;
+    std::vector<int> sa, sb;         // shell indices of the two functions
+    simint_multi_shellpair P;        // host pair data (Schwarz screened)
+    DevBuf dev;                      // packed records + sorted order
+    PairSetDev view;
+    std::vector<double> Q;           // Schwarz bound per pair
+    std::vector<int> order;          // pair indices by decreasing Q
+    const int * dorder = nullptr;
+};
+
+struct QClass
+{
+    int bx = 0, ky = 0;              // pair classes of bra and ket
+    int req[4];
+    long long ntask = 0, nprimq = 0, nfull = 0;
+    int nout = 0;
+    long long offset = 0;
+    std::vector<long long> prefix;   // nb + 1
+    std::vector<int> border;         // bra pair of each b
+    DevBuf dev;                      // prefix, border
+};
+
+__global__ void k_checksum(const double * __restrict__ v, long long n, double * __restrict__ sums)
+{
+    double s = 0.0, a = 0.0;
+    for(long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+        i += (long long)gridDim.x * blockDim.x)
+    {
+        const double x = v[i];
+        s += x;
+        a += fabs(x);
+    }
+    for(int o = 16; o > 0; o >>= 1)
+    {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        a += __shfl_down_sync(0xffffffffu, a, o);
+    }
+    if((threadIdx.x & 31) == 0)
+    {
+        atomicAdd(sums, s);
+        atomicAdd(sums + 1, a);
+    }
+}
+
+// primitive quartets that survive the reference's primitive screening
+template<int MODE>
+__global__ void k_count_primq(const KernArgs a, unsigned long long * count)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int iP, iQ;
+    long long off;
+    unsigned long long n = 0;
+    if(task_of<MODE>(a, t, iP, iQ, off))
+    {
+        QuartetCtx c;
+        make_ctx(a, iP, iQ, c);
+        for(int i = c.bi0; i < c.bi1; ++i)
+        {
+            const BraPrim bp = load_bra_prim(c, i);
+            if(c.check && bp.skip)
+                continue;
+            if(!c.check)
+            {
+                n += c.kj1 - c.kj0;
+                continue;
+            }
+            for(int j = c.kj0; j < c.kj1; ++j)
+                n += prim_survives(c, bp, j) ? 1 : 0;
+        }
+    }
+    for(int o = 16; o > 0; o >>= 1)
+        n += __shfl_down_sync(0xffffffffu, n, o);
+    if((threadIdx.x & 31) == 0 && n)
+        atomicAdd(count, n);
+}
+
+} // namespace
+
+struct simint_b200_basis
+{
+    int nshell = 0;
+    double tol = 0.0;
+    std::vector<simint_shell> shells;      // copies (storage owned by caller)
+    std::vector<PairClass> pcs;
+    std::vector<QClass> qcs;
+    long long total_out = 0;
+    DevBuf dsums;
+    std::map<std::array<long long, 3>, cudaGraphExec_t> graphs;
+    std::map<std::array<long long, 3>, int> eager_done;
+    cudaStream_t own_stream = nullptr;
+    int nlaunch = 0;
+};
+
+static void fill_args(const simint_b200_basis * b, const QClass & q, KernArgs & a);
+
+static void layout_outputs(simint_b200_basis * b)
+{
+    b->total_out = 0;
+    for(auto & q : b->qcs)
+    {
+        q.offset = b->total_out;
+        b->total_out += q.ntask * q.nout;
+    }
+}
+
+static int upload_tasks(QClass & q)
+{
+    const size_t szp = (q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255;
+    if(!q.dev.reserve(szp + q.border.size() * sizeof(int) + 8))
+    {
+        set_error("out of memory building task lists");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    cudaMemcpy(q.dev.ptr, q.prefix.data(), q.prefix.size() * sizeof(long long), cudaMemcpyHostToDevice);
+    cudaMemcpy((char *)q.dev.ptr + szp, q.border.data(), q.border.size() * sizeof(int), cudaMemcpyHostToDevice);
+    return 0;
+}
+
+static void fill_args(const simint_b200_basis * b, const QClass & q, KernArgs & a)
+{
+    memset(&a, 0, sizeof(a));
+    const PairClass & X = b->pcs[q.bx];
+    const PairClass & Y = b->pcs[q.ky];
+    a.P = X.view;
+    a.Q = Y.view;
+    a.check = b->tol > 0.0;
+    a.tol2 = b->tol * b->tol;
+    a.nout = q.nout;
+    a.prefix = (const long long *)q.dev.ptr;
+    a.border = (const int *)((const char *)q.dev.ptr + ((q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255));
+    a.korder = Y.dorder;
+    a.nb = (int)q.border.size();
+}
+
+extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simint_shell const * shells,
+                                                        double screen_tol, int max_am)
+{
+    init_tables();
+    if(ensure_device() < 0)
+        return nullptr;
+    if(nshell <= 0 || !shells || max_am < 0 || max_am > SIMINT_OSTEI_MAXAM)
+    {
+        set_error("bad argument to simint_b200_basis_create");
+        return nullptr;
+    }
+    simint_b200_basis * b = new simint_b200_basis;
+    b->nshell = nshell;
+    b->tol = screen_tol;
+    b->shells.assign(shells, shells + nshell);
+    Workspace & w = workspace();
+    if(!w.stream)
+        cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking);
+    std::vector<std::vector<int>> byam(max_am + 1);
+    for(int s = 0; s < nshell; s++)
+        if(shells[s].am <= max_am)
+            byam[shells[s].am].push_back(s);
+    // pair classes
+    for(int la = 0; la <= max_am; la++)
+        for(int lb = 0; lb <= la; lb++)
+        {
+            if(byam[la].empty() || byam[lb].empty())
+                continue;
+            PairClass pc;
+            pc.la = la;
+            pc.lb = lb;
+            for(int i : byam[la])
+                for(int j : byam[lb])
+                {
+                    if(la == lb && j > i)
+                        continue;
+                    pc.sa.push_back(i);
+                    pc.sb.push_back(j);
+                }
+            b->pcs.push_back(std::move(pc));
+        }
+    for(auto & pc : b->pcs)
+    {
+        const int n = (int)pc.sa.size();
+        std::vector<simint_shell> AB(2 * (size_t)n);
+        for(int k = 0; k < n; k++)
+        {
+            AB[2 * k] = shells[pc.sa[k]];
+            AB[2 * k + 1] = shells[pc.sb[k]];
+        }
+        simint_initialize_multi_shellpair(&pc.P);
+        simint_create_multi_shellpair2(n, AB.data(), &pc.P,
+                                       screen_tol > 0.0 ? SIMINT_SCREEN_SCHWARZ : SIMINT_SCREEN_NONE);
+        PackedLayout L;
+        const size_t sz = (pack_pairs(&pc.P, nullptr, L) + 255) & ~(size_t)255;
+        const size_t szo = ((size_t)n * sizeof(int) + 255) & ~(size_t)255;
+        const size_t szq = (size_t)n * sizeof(double);
+        if(!pc.dev.reserve(sz + szo + szq) || !w.hstage.reserve(sz))
+        {
+            set_error("out of memory building the basis");
+            simint_b200_basis_free(b);
+            return nullptr;
+        }
+        pack_pairs(&pc.P, (char *)w.hstage.ptr, L);
+        cudaMemcpy(pc.dev.ptr, w.hstage.ptr, sz, cudaMemcpyHostToDevice);
+        pc.view = device_view((const char *)pc.dev.ptr, L, pc.P.screen_max);
+        // Schwarz bound of every contracted pair
+        double * dq = (double *)((char *)pc.dev.ptr + sz + szo);
+        if(pair_diag_max(pc.view, pc.la, pc.lb, n, dq, w.stream) != 0)
+        {
+            simint_b200_basis_free(b);
+            return nullptr;
+        }
+        pc.Q.resize(n);
+        cudaMemcpy(pc.Q.data(), dq, n * sizeof(double), cudaMemcpyDeviceToHost);
+        for(auto & v : pc.Q)
+            v = std::sqrt(v);
+        pc.order.resize(n);
+        std::iota(pc.order.begin(), pc.order.end(), 0);
+        std::stable_sort(pc.order.begin(), pc.order.end(), [&](int x, int y) { return pc.Q[x] > pc.Q[y]; });
+        cudaMemcpy((char *)pc.dev.ptr + sz, pc.order.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+        pc.dorder = (const int *)((char *)pc.dev.ptr + sz);
+    }
+    // quartet classes: bra class >= ket class in (la+lb, la) order
+    std::vector<int> cls(b->pcs.size());
+    std::iota(cls.begin(), cls.end(), 0);
+    std::stable_sort(cls.begin(), cls.end(), [&](int x, int y) {
+        const auto & X = b->pcs[x];
+        const auto & Y = b->pcs[y];
+        return std::make_pair(X.la + X.lb, X.la) > std::make_pair(Y.la + Y.lb, Y.la);
+    });
+    for(size_t xi = 0; xi < cls.size(); xi++)
+        for(size_t yi = xi; yi < cls.size(); yi++)
+        {
+            QClass q;
+            q.bx = cls[xi];
+            q.ky = cls[yi];
+            const PairClass & X = b->pcs[q.bx];
+            const PairClass & Y = b->pcs[q.ky];
+            q.req[0] = X.la; q.req[1] = X.lb; q.req[2] = Y.la; q.req[3] = Y.lb;
+            q.nout = ncart_of(X.la) * ncart_of(X.lb) * ncart_of(Y.la) * ncart_of(Y.lb);
+            std::vector<double> qy(Y.order.size());
+            for(size_t k = 0; k < qy.size(); k++)
+                qy[k] = Y.Q[Y.order[k]];
+            long long tot = 0;
+            q.prefix.push_back(0);
+            for(size_t bb = 0; bb < X.order.size(); bb++)
+            {
+                const double qb = X.Q[X.order[bb]];
+                // ket pairs with qb * q >= tol: a prefix of the decreasing list
+                long long cut = (long long)qy.size();
+                if(screen_tol > 0.0)
+                {
+                    cut = std::upper_bound(qy.begin(), qy.end(), screen_tol / std::max(qb, 1e-300),
+                                           [](double t, double v) { return v < t; }) - qy.begin();
+                    // exact test at the boundary (division rounding)
+                    while(cut > 0 && qb * qy[cut - 1] < screen_tol) cut--;
+                    while(cut < (long long)qy.size() && qb * qy[cut] >= screen_tol) cut++;
+                }
+                long long cnt = (q.bx == q.ky) ? std::min<long long>((long long)bb + 1, cut) : cut;
+                if(cnt <= 0)
+                    continue;
+                q.border.push_back(X.order[bb]);
+                tot += cnt;
+                q.prefix.push_back(tot);
+            }
+            q.ntask = tot;
+            q.nfull = tot;
+            if(tot == 0)
+                continue;
+            if(upload_tasks(q) != 0)
+            {
+                simint_b200_basis_free(b);
+                return nullptr;
+            }
+            b->qcs.push_back(std::move(q));
+        }
+    layout_outputs(b);
+    if(!b->dsums.reserve(2 * sizeof(double) * std::max<size_t>(1, b->qcs.size())))
+    {
+        simint_b200_basis_free(b);
+        return nullptr;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("CUDA error building the basis: ") + cudaGetErrorString(e));
+        simint_b200_basis_free(b);
+        return nullptr;
+    }
+    return b;
+}
+
+extern "C" int simint_b200_basis_subsample(simint_b200_basis * b, long long maxq)
+{
+    if(!b || maxq <= 0)
+        return SIMINT_B200_ERR_ARG;
+    for(auto & g : b->graphs)
+        cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+    b->eager_done.clear();
+    for(auto & q : b->qcs)
+    {
+        if(q.ntask <= maxq)
+            continue;
+        const long long stride = (q.ntask + maxq - 1) / maxq;
+        std::vector<long long> pre(1, 0);
+        std::vector<int> bor;
+        const int nb = (int)q.border.size();
+        for(int r = 0; r < nb; r += (int)stride)
+        {
+            bor.push_back(q.border[r]);
+            pre.push_back(pre.back() + (q.prefix[r + 1] - q.prefix[r]));
+        }
+        q.prefix.swap(pre);
+        q.border.swap(bor);
+        q.ntask = q.prefix.back();
+        q.nprimq = 0;
+        if(upload_tasks(q) != 0)
+            return SIMINT_B200_ERR_CUDA;
+    }
+    layout_outputs(b);
+    return 0;
+}
+
+extern "C" int simint_b200_basis_nrows(simint_b200_basis const * b, int k)
+{
+    if(!b || k < 0 || k >= (int)b->qcs.size())
+        return SIMINT_B200_ERR_ARG;
+    return (int)b->qcs[k].border.size();
+}
+
+extern "C" int simint_b200_basis_row(simint_b200_basis const * b, int k, int r,
+                                     long long * first, long long * n)
+{
+    if(!b || k < 0 || k >= (int)b->qcs.size() || r < 0 || r >= (int)b->qcs[k].border.size())
+        return SIMINT_B200_ERR_ARG;
+    *first = b->qcs[k].prefix[r];
+    *n = b->qcs[k].prefix[r + 1] - b->qcs[k].prefix[r];
+    return 0;
+}
+
+extern "C" int simint_b200_basis_subsample_stride(simint_b200_basis * b, int stride, int offset)
+{
+    if(!b || stride < 1 || offset < 0)
+        return SIMINT_B200_ERR_ARG;
+    for(auto & g : b->graphs)
+        cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+    b->eager_done.clear();
+    for(auto & q : b->qcs)
+    {
+        std::vector<long long> pre(1, 0);
+        std::vector<int> bor;
+        const int nb = (int)q.border.size();
+        for(int r = offset % stride; r < nb; r += stride)
+        {
+            bor.push_back(q.border[r]);
+            pre.push_back(pre.back() + (q.prefix[r + 1] - q.prefix[r]));
+        }
+        q.prefix.swap(pre);
+        q.border.swap(bor);
+        q.ntask = q.prefix.back();
+        q.nprimq = 0;
+        if(upload_tasks(q) != 0)
+            return SIMINT_B200_ERR_CUDA;
+    }
+    layout_outputs(b);
+    return 0;
+}
+
+extern "C" long long simint_b200_basis_class_full(simint_b200_basis const * b, int k)
+{
+    if(k < 0 || k >= (int)b->qcs.size())
+        return SIMINT_B200_ERR_ARG;
+    return b->qcs[k].nfull;
+}
+
+extern "C" long long simint_b200_basis_count_primq(simint_b200_basis * b)
+{
+    unsigned long long * dcount = nullptr;
+    if(cudaMalloc(&dcount, sizeof(unsigned long long)) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    long long tot = 0;
+    for(auto & q : b->qcs)
+    {
+        KernArgs a;
+        fill_args(b, q, a);
+        a.ntask = q.ntask;
+        cudaMemset(dcount, 0, sizeof(unsigned long long));
+        k_count_primq<2><<<(unsigned)((q.ntask + 127) / 128), 128>>>(a, dcount);
+        unsigned long long c = 0;
+        cudaMemcpy(&c, dcount, sizeof(c), cudaMemcpyDeviceToHost);
+        q.nprimq = (long long)c;
+        tot += q.nprimq;
+    }
+    cudaFree(dcount);
+    return tot;
+}
+
+extern "C" void simint_b200_basis_free(simint_b200_basis * b)
+{
+    if(!b)
+        return;
+    for(auto & g : b->graphs)
+        cudaGraphExecDestroy(g.second);
+    for(auto & pc : b->pcs)
+    {
+        simint_free_multi_shellpair(&pc.P);
+        pc.dev.release();
+    }
+    for(auto & q : b->qcs)
+        q.dev.release();
+    b->dsums.release();
+    delete b;
+}
+
+extern "C" long long simint_b200_basis_nquartets(simint_b200_basis const * b)
+{
+    long long n = 0;
+    for(auto & q : b->qcs) n += q.ntask;
+    return n;
+}
+
+extern "C" long long simint_b200_basis_nprimquartets(simint_b200_basis const * b)
+{
+    long long n = 0;
+    for(auto & q : b->qcs) n += q.nprimq;
+    return n;
+}
+
+extern "C" long long simint_b200_basis_output_size(simint_b200_basis const * b)
+{
+    return b->total_out;
+}
+
+extern "C" int simint_b200_basis_nclass(simint_b200_basis const * b)
+{
+    return (int)b->qcs.size();
+}
+
+extern "C" int simint_b200_basis_class_info(simint_b200_basis const * b, int k, int am[4],
+                                            long long * nquart, long long * nprimq,
+                                            int * nout, long long * offset)
+{
+    if(k < 0 || k >= (int)b->qcs.size())
+        return SIMINT_B200_ERR_ARG;
+    const QClass & q = b->qcs[k];
+    if(am) memcpy(am, q.req, sizeof(q.req));
+    if(nquart) *nquart = q.ntask;
+    if(nprimq) *nprimq = q.nprimq;
+    if(nout) *nout = q.nout;
+    if(offset) *offset = q.offset;
+    return 0;
+}
+
+extern "C" int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long t, int sh[4])
+{
+    if(k < 0 || k >= (int)b->qcs.size() || t < 0 || t >= b->qcs[k].ntask)
+        return SIMINT_B200_ERR_ARG;
+    const QClass & q = b->qcs[k];
+    const int bi = (int)(std::upper_bound(q.prefix.begin(), q.prefix.end(), t) - q.prefix.begin()) - 1;
+    const int ip = q.border[bi];
+    const PairClass & X = b->pcs[q.bx];
+    const PairClass & Y = b->pcs[q.ky];
+    const int iq = Y.order[(size_t)(t - q.prefix[bi])];
+    sh[0] = X.sa[ip]; sh[1] = X.sb[ip];
+    sh[2] = Y.sa[iq]; sh[3] = Y.sb[iq];
+    return 0;
+}
+
+// Issue every launch of one sweep on `stream`.  events: optional per-class
+// start/stop pairs (eager runs only).
+static int issue_sweep(simint_b200_basis * b, int prec, double * dout, long long cap,
+                       cudaStream_t stream, cudaEvent_t * events)
+{
+    int nl = 0;
+    const bool full = cap >= b->total_out;
+    double * dsums = (double *)b->dsums.ptr;
+    cudaMemsetAsync(dsums, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        QClass & q = b->qcs[k];
+        if(events)
+            cudaEventRecord(events[2 * k], stream);
+        const long long chunk = full ? q.ntask : std::max<long long>(1, cap / q.nout);
+        for(long long t0 = 0; t0 < q.ntask; t0 += chunk)
+        {
+            const long long cn = std::min(chunk, q.ntask - t0);
+            KernArgs a;
+            fill_args(b, q, a);
+            a.ntask = cn;
+            a.task0 = t0;
+            a.out = full ? dout + q.offset + t0 * q.nout : dout;
+            a.gate = gate();
+            int rc = launch_class(a, q.req, 0, 2, prec, stream);
+            if(rc != 0)
+                return rc;
+            nl++;
+            const long long n = cn * q.nout;
+            const unsigned blocks = (unsigned)std::min<long long>(148 * 8, (n + 255) / 256);
+            k_checksum<<<blocks, 256, 0, stream>>>(a.out, n, dsums + 2 * k);
+            count_launch(1);
+            nl++;
+        }
+        if(events)
+            cudaEventRecord(events[2 * k + 1], stream);
+    }
+    return nl;
+}
+
+extern "C" int simint_b200_basis_compute(simint_b200_basis * b, int prec, double * dev_out,
+                                         long long dev_out_doubles, void * stream_)
+{
+    if(!b || !dev_out || dev_out_doubles <= 0)
+        return SIMINT_B200_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    const std::array<long long, 3> key = {prec, (long long)(uintptr_t)dev_out, dev_out_doubles};
+    auto it = b->graphs.find(key);
+    if(it != b->graphs.end())
+    {
+        if(cudaGraphLaunch(it->second, stream) != cudaSuccess)
+        {
+            set_error("cudaGraphLaunch failed");
+            return SIMINT_B200_ERR_CUDA;
+        }
+        count_launch(b->nlaunch);
+        return b->nlaunch;
+    }
+    if(!b->eager_done.count(key))
+    {
+        // first use: run eagerly so every table and scratch buffer exists
+        int nl = issue_sweep(b, prec, dev_out, dev_out_doubles, stream, nullptr);
+        if(nl < 0)
+            return nl;
+        b->eager_done[key] = 1;
+        b->nlaunch = nl;
+        return nl;
+    }
+    // second use: capture the sweep into a CUDA graph and replay it
+    cudaStream_t cs = stream;
+    bool own = false;
+    if(!cs)
+    {
+        cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        own = true;
+    }
+    cudaGraph_t graph;
+    if(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    {
+        set_error("cudaStreamBeginCapture failed");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    const long long before = simint_b200_launch_count();
+    int nl = issue_sweep(b, prec, dev_out, dev_out_doubles, cs, nullptr);
+    count_launch(-(simint_b200_launch_count() - before));   // captured, not launched
+    cudaError_t e = cudaStreamEndCapture(cs, &graph);
+    if(nl < 0)
+        return nl;
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("graph capture failed: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("graph instantiate failed: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    b->graphs[key] = exec;
+    if(own)
+    {
+        cudaStreamSynchronize(cs);
+        cudaStreamDestroy(cs);
+    }
+    b->nlaunch = nl;
+    cudaGraphLaunch(exec, stream);
+    count_launch(nl);
+    return nl;
+}
+
+extern "C" int simint_b200_basis_checksums(simint_b200_basis * b, double * sums)
+{
+    cudaDeviceSynchronize();
+    if(cudaMemcpy(sums, b->dsums.ptr, 2 * sizeof(double) * b->qcs.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    return 0;
+}
+
+extern "C" int simint_b200_basis_class_times(simint_b200_basis * b, int prec, double * dev_out,
+                                             long long dev_out_doubles, void * stream_, float * ms)
+{
+    cudaStream_t stream = (cudaStream_t)stream_;
+    std::vector<cudaEvent_t> ev(2 * b->qcs.size());
+    for(auto & e : ev)
+        cudaEventCreate(&e);
+    int nl = issue_sweep(b, prec, dev_out, dev_out_doubles, stream, ev.data());
+    cudaStreamSynchronize(stream);
+    for(size_t k = 0; k < b->qcs.size() && nl >= 0; k++)
+        cudaEventElapsedTime(&ms[k], ev[2 * k], ev[2 * k + 1]);
+    for(auto & e : ev)
+        cudaEventDestroy(e);
+    return nl;
+}

@@ -81,6 +81,20 @@ def make_pairs(lib, shells, pairs, screen=SIMINT_SCREEN_NONE):
     return P
 
 
+def count_primq(P, Q, screen_tol, lib=None):
+    lib = lib or load()
+    lib.simint_b200_count_primq.argtypes = [PairP, PairP, C.c_double]
+    lib.simint_b200_count_primq.restype = C.c_longlong
+    return lib.simint_b200_count_primq(C.byref(P), C.byref(Q), screen_tol)
+
+
+def fma_peak(fp32=False, lib=None):
+    lib = lib or load()
+    lib.simint_b200_fma_peak.argtypes = [C.c_int]
+    lib.simint_b200_fma_peak.restype = C.c_double
+    return lib.simint_b200_fma_peak(1 if fp32 else 0)
+
+
 def compute_eri(P, Q, screen_tol=0.0, deriv=0, lib=None):
     """simint_compute_eri(_deriv) into a fresh numpy array.
 
@@ -93,3 +107,133 @@ def compute_eri(P, Q, screen_tol=0.0, deriv=0, lib=None):
     if r < -1:
         raise RuntimeError("simint_compute_eri_deriv failed (%d): %s" % (r, last_error()))
     return r, out
+
+
+class Basis:
+    """simint_b200_basis: a device-resident, Schwarz-screened sweep."""
+
+    def __init__(self, shells, screen_tol, max_am=4, lib=None):
+        self.lib = lib or load()
+        L = self.lib
+        L.simint_b200_basis_create.argtypes = [C.c_int, ShellP, C.c_double, C.c_int]
+        L.simint_b200_basis_create.restype = C.c_void_p
+        L.simint_b200_basis_free.argtypes = [C.c_void_p]
+        L.simint_b200_basis_nquartets.argtypes = [C.c_void_p]
+        L.simint_b200_basis_nquartets.restype = C.c_longlong
+        L.simint_b200_basis_nprimquartets.argtypes = [C.c_void_p]
+        L.simint_b200_basis_nprimquartets.restype = C.c_longlong
+        L.simint_b200_basis_output_size.argtypes = [C.c_void_p]
+        L.simint_b200_basis_output_size.restype = C.c_longlong
+        L.simint_b200_basis_nclass.argtypes = [C.c_void_p]
+        L.simint_b200_basis_class_info.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                                   C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                                   C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+        L.simint_b200_basis_quartet.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.POINTER(C.c_int)]
+        L.simint_b200_basis_compute.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong, C.c_void_p]
+        L.simint_b200_basis_checksums.argtypes = [C.c_void_p, _dp]
+        L.simint_b200_basis_class_times.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong,
+                                                    C.c_void_p, C.POINTER(C.c_float)]
+        self.shells = shells
+        self.h = L.simint_b200_basis_create(shells.n, shells.ptr(0), screen_tol, max_am)
+        if not self.h:
+            raise RuntimeError("simint_b200_basis_create failed: " + last_error())
+
+    def close(self):
+        if self.h:
+            self.lib.simint_b200_basis_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nquartets(self):
+        return self.lib.simint_b200_basis_nquartets(self.h)
+
+    @property
+    def nprimquartets(self):
+        return self.lib.simint_b200_basis_nprimquartets(self.h)
+
+    @property
+    def output_size(self):
+        return self.lib.simint_b200_basis_output_size(self.h)
+
+    def classes(self):
+        out = []
+        for k in range(self.lib.simint_b200_basis_nclass(self.h)):
+            am = (C.c_int * 4)()
+            nq, npq, off = C.c_longlong(), C.c_longlong(), C.c_longlong()
+            nout = C.c_int()
+            self.lib.simint_b200_basis_class_info(self.h, k, am, C.byref(nq), C.byref(npq),
+                                                  C.byref(nout), C.byref(off))
+            out.append(dict(am=tuple(am), nquart=nq.value, nprimq=npq.value,
+                            nout=nout.value, offset=off.value))
+        return out
+
+    def subsample(self, max_quartets):
+        L = self.lib
+        L.simint_b200_basis_subsample.argtypes = [C.c_void_p, C.c_longlong]
+        r = L.simint_b200_basis_subsample(self.h, max_quartets)
+        if r != 0:
+            raise RuntimeError("subsample failed: " + last_error())
+
+    def subsample_stride(self, stride, offset=0):
+        self.lib.simint_b200_basis_subsample_stride.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        r = self.lib.simint_b200_basis_subsample_stride(self.h, stride, offset)
+        if r != 0:
+            raise RuntimeError("subsample_stride failed: " + last_error())
+
+    def rows(self, k):
+        """(first task, number of tasks) of every bra-pair row of class k."""
+        L = self.lib
+        L.simint_b200_basis_nrows.argtypes = [C.c_void_p, C.c_int]
+        L.simint_b200_basis_row.argtypes = [C.c_void_p, C.c_int, C.c_int,
+                                            C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        out = []
+        for r in range(L.simint_b200_basis_nrows(self.h, k)):
+            f, n = C.c_longlong(), C.c_longlong()
+            L.simint_b200_basis_row(self.h, k, r, C.byref(f), C.byref(n))
+            out.append((f.value, n.value))
+        return out
+
+    def class_full(self, k):
+        self.lib.simint_b200_basis_class_full.argtypes = [C.c_void_p, C.c_int]
+        self.lib.simint_b200_basis_class_full.restype = C.c_longlong
+        return self.lib.simint_b200_basis_class_full(self.h, k)
+
+    def count_primq(self):
+        self.lib.simint_b200_basis_count_primq.argtypes = [C.c_void_p]
+        self.lib.simint_b200_basis_count_primq.restype = C.c_longlong
+        return self.lib.simint_b200_basis_count_primq(self.h)
+
+    def quartet(self, k, q):
+        sh = (C.c_int * 4)()
+        r = self.lib.simint_b200_basis_quartet(self.h, k, q, sh)
+        if r != 0:
+            raise IndexError((k, q))
+        return tuple(sh)
+
+    def compute(self, prec, dev_ptr, ndoubles, stream=0):
+        r = self.lib.simint_b200_basis_compute(self.h, prec, C.c_void_p(dev_ptr), ndoubles,
+                                               C.c_void_p(stream))
+        if r < 0:
+            raise RuntimeError("simint_b200_basis_compute failed (%d): %s" % (r, last_error()))
+        return r
+
+    def checksums(self):
+        n = self.lib.simint_b200_basis_nclass(self.h)
+        s = np.zeros(2 * max(n, 1))
+        self.lib.simint_b200_basis_checksums(self.h, s.ctypes.data_as(_dp))
+        return s[:2 * n].reshape(n, 2)
+
+    def class_times(self, prec, dev_ptr, ndoubles, stream=0):
+        n = self.lib.simint_b200_basis_nclass(self.h)
+        ms = (C.c_float * max(n, 1))()
+        r = self.lib.simint_b200_basis_class_times(self.h, prec, C.c_void_p(dev_ptr), ndoubles,
+                                                   C.c_void_p(stream), ms)
+        if r < 0:
+            raise RuntimeError("class_times failed: " + last_error())
+        return list(ms)[:n]

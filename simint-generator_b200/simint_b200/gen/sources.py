@@ -49,7 +49,7 @@ def kernel_file(am):
     o.append("void register_%s(KernelTable & t)" % name)
     o.append("{")
     o.append("    ClassKernels k = {{%d, %d, %d, %d}, %d, %d, %d, %d," % (am + (p.L, ntop, p.vrr_flops(), p.hrr_flops())))
-    o.append("        {{k_%s<0,0>, k_%s<0,1>}, {k_%s<1,0>, k_%s<1,1>}}};" % ((name,) * 4))
+    o.append("        {{k_%s<0,0>, k_%s<0,1>}, {k_%s<1,0>, k_%s<1,1>}, {k_%s<2,0>, k_%s<2,1>}}};" % ((name,) * 6))
     o.append("    t.add(k);")
     o.append("}")
     return "\n".join(o) + "\n"
