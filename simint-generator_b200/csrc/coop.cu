@@ -59,10 +59,27 @@ struct CoopClass
 __device__ __forceinline__ int c_lev_off(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
 __device__ __forceinline__ int c_nc(int l) { return ((l + 1) * (l + 2)) / 2; }
 
+// Cartesian position in the output ordering, from the shared-memory table
+__device__ __forceinline__ int ci_index(const CartInfo * __restrict__ ci, int g, int ordering)
+{
+    const CartInfo & c = ci[g];
+    const int l = c.lev;
+    if(ordering == SIMINT_B200_ORDERING_GAMESS && (l == 2 || l == 3))
+    {
+        const int i = c.ijk[0], j = c.ijk[1], k = c.ijk[2];
+        if(l == 2)
+            return i == 2 ? 0 : j == 2 ? 1 : k == 2 ? 2 : (i == 1 && j == 1) ? 3 : i == 1 ? 4 : 5;
+        return i == 3 ? 0 : j == 3 ? 1 : k == 3 ? 2 : (i == 2 && j == 1) ? 3 : i == 2 ? 4
+             : (i == 1 && j == 2) ? 5 : j == 2 ? 6 : (i == 1 && k == 2) ? 7 : k == 2 ? 8 : 9;
+    }
+    return c.pos;
+}
+
 // one side of the HRR for one column, working array H in global scratch
 // (same recurrence as the oracle's hrr_side)
 template<typename SRC, typename DST>
-__device__ void coop_hrr_col(int right_step, int ta, int tb, const double X[3], SRC src, DST dst,
+__device__ void coop_hrr_col(const CartInfo * __restrict__ ci, int right_step, int ta, int tb,
+                             double X0, double X1, double X2, SRC src, DST dst,
                              double * __restrict__ H)
 {
     const int lt = ta + tb;
@@ -76,12 +93,13 @@ __device__ void coop_hrr_col(int right_step, int ta, int tb, const double X[3], 
             for(int it = c_lev_off(tl); it < c_lev_off(tl + 1); it++)
                 for(int is = c_lev_off(sl); is < c_lev_off(sl + 1); is++)
                 {
-                    const int x = c_cartinfo[is].dir;
-                    const int ism = c_cartinfo[is].m1[x];
-                    const int itp = c_cartinfo[it].p1[x];
+                    const int x = ci[is].dir;
+                    const int ism = ci[is].m1[x];
+                    const int itp = ci[it].p1[x];
                     const double a = H[it * nstep + ism];
                     const double b = H[itp * nstep + ism];
-                    H[it * nstep + is] = right_step ? fma(X[x], a, b) : fma(-X[x], a, b);
+                    const double X = x == 0 ? X0 : (x == 1 ? X1 : X2);
+                    H[it * nstep + is] = right_step ? fma(X, a, b) : fma(-X, a, b);
                 }
     for(int a = 0; a < c_nc(ta); a++)
         for(int b = 0; b < c_nc(tb); b++)
@@ -98,6 +116,10 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
                                               double * __restrict__ gscr)
 {
     extern __shared__ double sm[];
+    __shared__ CartInfo ci[CI_NCART];
+    for(int k = threadIdx.x; k < CI_NCART; k += blockDim.x)
+        ci[k] = c_cartinfo[k];
+    __syncthreads();
     double * wave = sm;                         // 3 * wsize
     double * acc = sm + 3 * gc.wsize;           // acc_size
     const int L = gc.L;
@@ -164,18 +186,17 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
                     }
                     wave[tid] = F[tid] * s.prefac;      // block (0,0), wavefront 0
                 }
-                const double XP[3] = {gc.brastep_j ? s.PAx : s.PBx, gc.brastep_j ? s.PAy : s.PBy,
-                                      gc.brastep_j ? s.PAz : s.PBz};
-                const double XQ[3] = {gc.ketstep_l ? s.QCx : s.QDx, gc.ketstep_l ? s.QCy : s.QDy,
-                                      gc.ketstep_l ? s.QCz : s.QDz};
-                const double aop[3] = {s.aopPQx, s.aopPQy, s.aopPQz};
-                const double aoq[3] = {s.aoqPQx, s.aoqPQy, s.aoqPQz};
-                const double w[5] = {1.0, s.c2a, s.c2b, s.c2c, s.c2d};
+                const double XP0 = gc.brastep_j ? s.PAx : s.PBx, XP1 = gc.brastep_j ? s.PAy : s.PBy,
+                             XP2 = gc.brastep_j ? s.PAz : s.PBz;
+                const double XQ0 = gc.ketstep_l ? s.QCx : s.QDx, XQ1 = gc.ketstep_l ? s.QCy : s.QDy,
+                             XQ2 = gc.ketstep_l ? s.QCz : s.QDz;
+#define SEL3(x, a, b, c) ((x) == 0 ? (a) : ((x) == 1 ? (b) : (c)))
+#define WTAG(tg) ((tg) == 0 ? 1.0 : ((tg) == 1 ? s.c2a : ((tg) == 2 ? s.c2b : ((tg) == 3 ? s.c2c : s.c2d))))
                 // (ss|ss) is a top when both target sides are s
                 if(tid == 0)
                     for(int tg = 0; tg < gc.ntag; tg++)
                         if(gc.elo[tg] == 0 && gc.flo[tg] == 0 && gc.ehi[tg] >= 0 && gc.fhi[tg] >= 0)
-                            acc[gc.acc_off[tg]] += (tg == 0 ? 1.0 : w[tg]) * wave[0];
+                            acc[gc.acc_off[tg]] += WTAG(tg) * wave[0];
                 __syncthreads();
                 for(int sfront = 1; sfront <= gc.Emax + gc.Fmax; sfront++)
                 {
@@ -203,49 +224,49 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
                         double v;
                         if(use_ket)
                         {
-                            const int x = c_cartinfo[gF].dir;
-                            const int gF1 = c_cartinfo[gF].m1[x];
-                            const int nfx = c_cartinfo[gF].ijk[x];
-                            const int gE1 = c_cartinfo[gE].m1[x];
+                            const int x = ci[gF].dir;
+                            const int gF1 = ci[gF].m1[x];
+                            const int nfx = ci[gF].ijk[x];
+                            const int gE1 = ci[gE].m1[x];
                             const int mlen1 = mlen + 1, mlen2 = mlen + 2;
                             // (e, f-1) in s-1
-                            const double * b1 = w1 + gc.boff[e][f - 1] + (pe * c_nc(f - 1) + c_cartinfo[gF1].pos) * mlen1;
-                            v = XQ[x] * b1[m];
-                            v = fma(aoq[x], b1[m + 1], v);
+                            const double * b1 = w1 + gc.boff[e][f - 1] + (pe * c_nc(f - 1) + ci[gF1].pos) * mlen1;
+                            v = SEL3(x, XQ0, XQ1, XQ2) * b1[m];
+                            v = fma(SEL3(x, s.aoqPQx, s.aoqPQy, s.aoqPQz), b1[m + 1], v);
                             if(nfx >= 2)
                             {
-                                const int gF2 = c_cartinfo[gF].m2;
-                                const double * b2 = w2 + gc.boff[e][f - 2] + (pe * c_nc(f - 2) + c_cartinfo[gF2].pos) * mlen2;
+                                const int gF2 = ci[gF].m2;
+                                const double * b2 = w2 + gc.boff[e][f - 2] + (pe * c_nc(f - 2) + ci[gF2].pos) * mlen2;
                                 v = fma((double)(nfx - 1) * s.oo2q, fma(s.a_over_q, b2[m + 1], b2[m]), v);
                             }
                             if(gE1 >= 0)
                             {
                                 const double * b3 = w2 + gc.boff[e - 1][f - 1]
-                                                    + (c_cartinfo[gE1].pos * c_nc(f - 1) + c_cartinfo[gF1].pos) * mlen2;
-                                v = fma((double)c_cartinfo[gE].ijk[x] * s.oo2pq, b3[m + 1], v);
+                                                    + (ci[gE1].pos * c_nc(f - 1) + ci[gF1].pos) * mlen2;
+                                v = fma((double)ci[gE].ijk[x] * s.oo2pq, b3[m + 1], v);
                             }
                         }
                         else
                         {
-                            const int x = c_cartinfo[gE].dir;
-                            const int gE1 = c_cartinfo[gE].m1[x];
-                            const int nex = c_cartinfo[gE].ijk[x];
-                            const int gF1 = c_cartinfo[gF].m1[x];
+                            const int x = ci[gE].dir;
+                            const int gE1 = ci[gE].m1[x];
+                            const int nex = ci[gE].ijk[x];
+                            const int gF1 = ci[gF].m1[x];
                             const int mlen1 = mlen + 1, mlen2 = mlen + 2;
-                            const double * b1 = w1 + gc.boff[e - 1][f] + (c_cartinfo[gE1].pos * c_nc(f) + pf) * mlen1;
-                            v = XP[x] * b1[m];
-                            v = fma(aop[x], b1[m + 1], v);
+                            const double * b1 = w1 + gc.boff[e - 1][f] + (ci[gE1].pos * c_nc(f) + pf) * mlen1;
+                            v = SEL3(x, XP0, XP1, XP2) * b1[m];
+                            v = fma(SEL3(x, s.aopPQx, s.aopPQy, s.aopPQz), b1[m + 1], v);
                             if(nex >= 2)
                             {
-                                const int gE2 = c_cartinfo[gE].m2;
-                                const double * b2 = w2 + gc.boff[e - 2][f] + (c_cartinfo[gE2].pos * c_nc(f) + pf) * mlen2;
+                                const int gE2 = ci[gE].m2;
+                                const double * b2 = w2 + gc.boff[e - 2][f] + (ci[gE2].pos * c_nc(f) + pf) * mlen2;
                                 v = fma((double)(nex - 1) * s.oo2p, fma(s.a_over_p, b2[m + 1], b2[m]), v);
                             }
                             if(gF1 >= 0)
                             {
                                 const double * b3 = w2 + gc.boff[e - 1][f - 1]
-                                                    + (c_cartinfo[gE1].pos * c_nc(f - 1) + c_cartinfo[gF1].pos) * mlen2;
-                                v = fma((double)c_cartinfo[gF].ijk[x] * s.oo2pq, b3[m + 1], v);
+                                                    + (ci[gE1].pos * c_nc(f - 1) + ci[gF1].pos) * mlen2;
+                                v = fma((double)ci[gF].ijk[x] * s.oo2pq, b3[m + 1], v);
                             }
                         }
                         cur[gc.boff[e][f] + pp * mlen + m] = v;
@@ -255,7 +276,7 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
                                 {
                                     const int re = gE - c_lev_off(gc.elo[tg]);
                                     const int rf = gF - c_lev_off(gc.flo[tg]);
-                                    acc[gc.acc_off[tg] + re * gc.acc_nf[tg] + rf] += (tg == 0 ? v : v * w[tg]);
+                                    acc[gc.acc_off[tg] + re * gc.acc_nf[tg] + rf] += (tg == 0 ? v : v * WTAG(tg));
                                 }
                     }
                     __syncthreads();
@@ -276,7 +297,7 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
             {
                 if(col < c_lev_off(flo))
                     continue;     // ket levels below the accumulated range are never read
-                coop_hrr_col(gc.brastep_j, tt[0], tt[1], c.AB,
+                coop_hrr_col(ci, gc.brastep_j, tt[0], tt[1], c.AB[0], c.AB[1], c.AB[2],
                              [&](int g) { return acc[gc.acc_off[tg] + (g - c_lev_off(elo)) * gc.acc_nf[tg]
                                                      + (col - c_lev_off(flo))]; },
                              [&](int r, double v) { bra[r * ncolF + col] = v; }, Hth);
@@ -284,7 +305,7 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
             __syncthreads();
             double * res = cta + gc.cta_res[ti];
             for(int r = tid; r < nbra; r += nth)
-                coop_hrr_col(gc.ketstep_l, tt[2], tt[3], c.CD,
+                coop_hrr_col(ci, gc.ketstep_l, tt[2], tt[3], c.CD[0], c.CD[1], c.CD[2],
                              [&](int g) { return bra[r * ncolF + g]; },
                              [&](int k, double v) { res[r * nket + k] = v; }, Hth);
             __syncthreads();
@@ -299,8 +320,8 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
             const int pd = idx % n3, pc = (idx / n3) % n2, pb = (idx / (n3 * n2)) % n1, pa = idx / (n3 * n2 * n1);
             const int ga = c_lev_off(am[0]) + pa, gb = c_lev_off(am[1]) + pb;
             const int gcc = c_lev_off(am[2]) + pc, gd = c_lev_off(am[3]) + pd;
-            const int oi = ((cart_index_dev(ga, gc.ordering) * n1 + cart_index_dev(gb, gc.ordering)) * n2
-                            + cart_index_dev(gcc, gc.ordering)) * n3 + cart_index_dev(gd, gc.ordering);
+            const int oi = ((ci_index(ci, ga, gc.ordering) * n1 + ci_index(ci, gb, gc.ordering)) * n2
+                            + ci_index(ci, gcc, gc.ordering)) * n3 + ci_index(ci, gd, gc.ordering);
             if(gc.deriv == 0)
             {
                 o[oi] = cta[gc.cta_res[0] + idx];
@@ -321,18 +342,18 @@ __global__ void __launch_bounds__(128) k_coop(const KernArgs a, const CoopClass 
                 for(int x = 0; x < 3; x++)
                 {
                     int h[4] = {gg[0], gg[1], gg[2], gg[3]};
-                    h[ctr] = c_cartinfo[gg[ctr]].p1[x];
+                    h[ctr] = ci[gg[ctr]].p1[x];
                     const int * tp_am = gc.tgt[tp];
-                    int r = ((c_cartinfo[h[0]].pos * c_nc(tp_am[1]) + c_cartinfo[h[1]].pos) * c_nc(tp_am[2])
-                             + c_cartinfo[h[2]].pos) * c_nc(tp_am[3]) + c_cartinfo[h[3]].pos;
+                    int r = ((ci[h[0]].pos * c_nc(tp_am[1]) + ci[h[1]].pos) * c_nc(tp_am[2])
+                             + ci[h[2]].pos) * c_nc(tp_am[3]) + ci[h[3]].pos;
                     double v = cta[gc.cta_res[tp] + r];
-                    const int nx = c_cartinfo[gg[ctr]].ijk[x];
+                    const int nx = ci[gg[ctr]].ijk[x];
                     if(nx > 0)
                     {
-                        h[ctr] = c_cartinfo[gg[ctr]].m1[x];
+                        h[ctr] = ci[gg[ctr]].m1[x];
                         const int * tm_am = gc.tgt[tm];
-                        r = ((c_cartinfo[h[0]].pos * c_nc(tm_am[1]) + c_cartinfo[h[1]].pos) * c_nc(tm_am[2])
-                             + c_cartinfo[h[2]].pos) * c_nc(tm_am[3]) + c_cartinfo[h[3]].pos;
+                        r = ((ci[h[0]].pos * c_nc(tm_am[1]) + ci[h[1]].pos) * c_nc(tm_am[2])
+                             + ci[h[2]].pos) * c_nc(tm_am[3]) + ci[h[3]].pos;
                         v -= nx * cta[gc.cta_res[tm] + r];
                     }
                     g12[ctr * 3 + x] = v;
