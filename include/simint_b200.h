@@ -148,3 +148,47 @@ double simint_b200_fma_peak(int fp32);
 #ifdef __cplusplus
 }
 #endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------
+ * ERIs without any allocation (no counterpart in the reference).
+ *
+ * For callers that may not allocate device memory -- code inside a
+ * framework that owns the device memory pool and only hands out buffers,
+ * code that runs while such a pool is captured or frozen, or hot paths that
+ * must never trigger the implicit synchronisation of cudaMalloc/cudaFree.
+ *
+ * simint_b200_packed_size / simint_b200_pack write the packed pair layout
+ * of P into caller memory (host); the caller copies it to a device buffer it
+ * owns.  simint_b200_compute_eri_noalloc then computes the same integrals
+ * as simint_compute_eri_deriv(deriv, P, Q, ...) into the caller's device
+ * buffer dev_integrals, on `stream` (cudaStream_t; NULL = legacy stream),
+ * asynchronously.  It runs the cooperative kernel; its working memory is a
+ * file-scope static device array of simint_b200_noalloc_scratch_bytes()
+ * (32 MiB) that every GPU which loads the library holds until exit, plus
+ * static Boys tables and an identity ket order (at most 2^20 ket pairs).
+ * It calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * The first call on a device performs that device's set-up (resolves the
+ * static arrays with cudaGetSymbolAddress, uploads tables, synchronises the
+ * device), so make it before any stream capture.  All calls share the one
+ * scratch array, which keeps the last call's contents: calls that overlap
+ * on the GPU (different streams, threads or graphs) race and must be
+ * serialised by the caller.  Returns nshell12_clip(P)*nshell12_clip(Q),
+ * -1 when the pair-level test screens everything (nothing written), or a
+ * negative SIMINT_B200_ERR_* code: ERR_ARG also when one CTA's scratch
+ * would exceed the static array or Q has more than 2^20 pairs. */
+size_t simint_b200_packed_size(struct simint_multi_shellpair const * P);
+int simint_b200_pack(struct simint_multi_shellpair const * P, void * host_dst, size_t capacity);
+long long simint_b200_noalloc_scratch_bytes(void);
+int simint_b200_compute_eri_noalloc(int deriv,
+                                    struct simint_multi_shellpair const * P, const void * dev_P,
+                                    struct simint_multi_shellpair const * Q, const void * dev_Q,
+                                    double screen_tol, double * dev_integrals, void * stream);
+
+#ifdef __cplusplus
+}
+#endif

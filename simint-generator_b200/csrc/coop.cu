@@ -20,13 +20,16 @@
 
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "simint_b200.h"
 #include "runtime.h"
 #include "cartinfo.cuh"
+#include "gen/boys_grid.inc"
 
 #define CMAXL 10
 #define CMAXB 12            // blocks per wavefront (levels 0..E, <= CMAXL+1)
@@ -549,3 +552,250 @@ int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_
 }
 
 } // namespace sb200
+
+// ===========================================================================
+// Entry point that allocates nothing.
+//
+// Some callers cannot allocate device memory: code running inside a
+// framework that owns the whole device pool (it hands out buffers but
+// forbids cudaMalloc), code called while a memory pool is being captured or
+// frozen, or hosts that must never trigger a cudaMalloc/cudaFree (an
+// implicit device synchronisation) on their hot path.  For them the
+// cooperative kernel can run with every working array in memory that exists
+// from load time: its global scratch, the Boys tables and an identity ket
+// order live in file-scope static device arrays of fixed size.  The caller
+// provides the packed pair data and the output in its own device buffers.
+// ===========================================================================
+
+#define NOALLOC_SCRATCH_DOUBLES (4 * 1024 * 1024)   // 32 MiB of scratch per device
+#define NOALLOC_MAX_KETS (1 << 20)                  // identity ket order, 4 MiB
+#define NOALLOC_MAX_DEV 64
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+static __device__ __align__(256) int g_noalloc_kord[NOALLOC_MAX_KETS];
+static __device__ __align__(256) double g_noalloc_boys[366 * 32 + 32];
+
+__global__ void k_noalloc_iota(int * p, int n)
+{
+    for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        p[i] = i;
+}
+
+namespace {
+
+struct NoallocDev
+{
+    int ready = 0;
+    double * scratch = nullptr;
+    int * kord = nullptr;
+    double * boys = nullptr;
+};
+
+NoallocDev g_noalloc[NOALLOC_MAX_DEV];
+std::mutex g_noalloc_mutex;
+CartInfo g_noalloc_cart[CI_NCART];
+
+// Packed layout of one pair set (the same records simint_compute_eri
+// uploads, see ostei_device.cuh), computed without allocating.
+size_t noalloc_layout(const simint_multi_shellpair * P, sb200::PackedLayout & L)
+{
+    int idx = 0;
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        idx += P->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 || p + 1 >= P->nshell12)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    L.npad = idx;
+    L.npair = P->nshell12;
+    L.off_rec = 0;
+    L.off_start = (size_t)idx * SB_REC * sizeof(double);
+    L.off_nprim = L.off_start + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    L.off_AB = L.off_nprim + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    return L.off_AB + 3 * (size_t)P->nshell12 * sizeof(double);
+}
+
+// Per-device set-up: resolve the static arrays' device addresses, upload
+// the Boys and Cartesian tables, fill the identity ket order.
+int noalloc_setup(int dev)
+{
+    NoallocDev & d = g_noalloc[dev];
+    if(d.ready)
+        return 0;
+    if(cudaGetSymbolAddress((void **)&d.scratch, g_noalloc_scratch) != cudaSuccess ||
+       cudaGetSymbolAddress((void **)&d.kord, g_noalloc_kord) != cudaSuccess ||
+       cudaGetSymbolAddress((void **)&d.boys, g_noalloc_boys) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return SIMINT_B200_ERR_CUDA;
+    }
+    if(cudaMemcpyToSymbol(g_noalloc_boys, simint_b200_boys_grid_host, sizeof(double) * 366 * 32) != cudaSuccess ||
+       cudaMemcpyToSymbol(g_noalloc_boys, simint_b200_boys_longfac_host, sizeof(double) * 32,
+                          sizeof(double) * 366 * 32) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    for(int l = 0; l <= CI_MAXL; l++)
+    {
+        int p = 0;
+        for(int i = l; i >= 0; i--)
+            for(int j = l - i; j >= 0; j--, p++)
+            {
+                const int k = l - i - j;
+                CartInfo & c = g_noalloc_cart[ci_lev_off(l) + p];
+                c.ijk[0] = (signed char)i; c.ijk[1] = (signed char)j; c.ijk[2] = (signed char)k;
+                c.lev = (signed char)l;
+                c.pos = (signed char)p;
+                const int e[3] = {i, j, k};
+                int mn = 1000, dir = -1;
+                for(int x = 0; x < 3; x++)
+                    if(e[x] > 0 && e[x] < mn) mn = e[x];
+                for(int x = 2; x >= 0; x--)
+                    if(e[x] == mn) { dir = x; break; }
+                c.dir = (signed char)dir;
+                c.m1[0] = (short)ci_flat(i - 1, j, k);
+                c.m1[1] = (short)ci_flat(i, j - 1, k);
+                c.m1[2] = (short)ci_flat(i, j, k - 1);
+                c.p1[0] = (short)ci_flat(i + 1, j, k);
+                c.p1[1] = (short)ci_flat(i, j + 1, k);
+                c.p1[2] = (short)ci_flat(i, j, k + 1);
+                int q[3] = {i, j, k};
+                if(dir >= 0) q[dir] -= 2;
+                c.m2 = (short)(dir >= 0 ? ci_flat(q[0], q[1], q[2]) : -1);
+            }
+    }
+    if(cudaMemcpyToSymbol(c_cartinfo, g_noalloc_cart, sizeof(CartInfo) * CI_NCART) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    k_noalloc_iota<<<256, 256>>>(d.kord, NOALLOC_MAX_KETS);
+    if(cudaDeviceSynchronize() != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    if(cudaFuncSetAttribute(k_coop<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    d.ready = 1;
+    return 0;
+}
+
+} // namespace
+
+extern "C" size_t simint_b200_packed_size(struct simint_multi_shellpair const * P)
+{
+    sb200::PackedLayout L;
+    return noalloc_layout(P, L);
+}
+
+extern "C" int simint_b200_pack(struct simint_multi_shellpair const * P, void * dst, size_t cap)
+{
+    sb200::PackedLayout L;
+    const size_t need = noalloc_layout(P, L);
+    if(!P || !dst || cap < need)
+        return SIMINT_B200_ERR_ARG;
+    char * base = (char *)dst;
+    double * rec = (double *)(base + L.off_rec);
+    int * start = (int *)(base + L.off_start);
+    int idx = 0;
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        start[p] = idx;
+        idx += P->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 || p + 1 >= P->nshell12)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    const bool has_screen = P->screen != nullptr;
+    for(int s = 0; s < L.npad; s++)
+    {
+        double * r = rec + (size_t)s * SB_REC;
+        r[0] = P->alpha[s]; r[1] = P->prefac[s];
+        r[2] = P->x[s]; r[3] = P->y[s]; r[4] = P->z[s];
+        r[5] = P->PA_x[s]; r[6] = P->PA_y[s]; r[7] = P->PA_z[s];
+        r[8] = P->PB_x[s]; r[9] = P->PB_y[s]; r[10] = P->PB_z[s];
+        r[11] = P->alpha2 ? P->alpha2[s] : 0.0;
+        r[12] = P->beta2 ? P->beta2[s] : 0.0;
+        const double sc = has_screen ? P->screen[s] : 0.0;
+        r[13] = sc;
+        r[15] = has_screen ? sqrt(sc > 0.0 ? sc : 0.0) : INFINITY;
+    }
+    for(int g = 0; g < L.npad; g += 8)
+    {
+        double m = 0.0;
+        for(int s = g; s < g + 8 && s < L.npad; s++)
+            m = fmax(m, rec[(size_t)s * SB_REC + 13]);
+        for(int s = g; s < g + 8 && s < L.npad; s++)
+            rec[(size_t)s * SB_REC + 14] = m;
+    }
+    memcpy(base + L.off_nprim, P->nprim12, P->nshell12 * sizeof(int));
+    double * ab = (double *)(base + L.off_AB);
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        ab[3 * p + 0] = P->AB_x[p];
+        ab[3 * p + 1] = P->AB_y[p];
+        ab[3 * p + 2] = P->AB_z[p];
+    }
+    return 0;
+}
+
+extern "C" long long simint_b200_noalloc_scratch_bytes(void)
+{
+    return (long long)NOALLOC_SCRATCH_DOUBLES * (long long)sizeof(double);
+}
+
+extern "C" int simint_b200_compute_eri_noalloc(int deriv,
+                                              struct simint_multi_shellpair const * P, const void * dev_P,
+                                              struct simint_multi_shellpair const * Q, const void * dev_Q,
+                                              double screen_tol, double * dev_integrals, void * stream)
+{
+    if(!P || !Q || !dev_P || !dev_Q || !dev_integrals || deriv < 0 || deriv > 1)
+        return SIMINT_B200_ERR_ARG;
+    const double tol2 = screen_tol * screen_tol;
+    if(screen_tol > 0.0 && P->screen_max * Q->screen_max < tol2)
+        return -1;
+    const long long ntask = (long long)P->nshell12_clip * Q->nshell12_clip;
+    if(ntask == 0)
+        return 0;
+    if(Q->nshell12_clip > NOALLOC_MAX_KETS)
+        return SIMINT_B200_ERR_ARG;
+    const int req[4] = {P->am1, P->am2, Q->am1, Q->am2};
+    for(int k = 0; k < 4; k++)
+        if(req[k] < 0 || req[k] > SIMINT_OSTEI_MAXAM)
+            return SIMINT_B200_ERR_CLASS;
+    int dev = 0;
+    if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEV)
+        return SIMINT_B200_ERR_NODEVICE;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+        const int rc = noalloc_setup(dev);
+        if(rc != 0)
+            return rc;
+    }
+    const NoallocDev & d = g_noalloc[dev];
+    CoopClass g;
+    if(!sb200::coop_setup(req, deriv, g) || g.smem_doubles * 8 > 200 * 1024)
+        return SIMINT_B200_ERR_CLASS;
+    const int threads = 128;
+    const long long per_cta = (long long)threads * g.h_per_thread + g.cta_size;
+    const long long max_cta = NOALLOC_SCRATCH_DOUBLES / per_cta;
+    if(max_cta < 1)
+        return SIMINT_B200_ERR_ARG;        // one CTA's scratch exceeds the static array
+    const int per_sm = std::max(1, std::min(8, (int)((220 * 1024) / std::max<size_t>((size_t)g.smem_doubles * 8, 1))));
+    long long grid = std::min<long long>(ntask, 148LL * per_sm);
+    grid = std::max<long long>(1, std::min(grid, max_cta));
+    sb200::PackedLayout LP, LQ;
+    noalloc_layout(P, LP);
+    noalloc_layout(Q, LQ);
+    KernArgs a;
+    memset(&a, 0, sizeof(a));
+    a.P = sb200::device_view((const char *)dev_P, LP, P->screen_max);
+    a.Q = sb200::device_view((const char *)dev_Q, LQ, Q->screen_max);
+    a.kord = d.kord;
+    a.ntask = ntask;
+    a.nQ = Q->nshell12_clip;
+    a.check = (screen_tol > 0.0) && P->screen && Q->screen;
+    a.tol2 = tol2;
+    a.out = dev_integrals;
+    a.nout = g.am[0] >= 0 ? (((req[0] + 1) * (req[0] + 2) / 2) * ((req[1] + 1) * (req[1] + 2) / 2)
+                             * ((req[2] + 1) * (req[2] + 2) / 2) * ((req[3] + 1) * (req[3] + 2) / 2)
+                             * (deriv ? 12 : 1)) : 0;
+    a.boys = d.boys;
+    const size_t smem = (size_t)g.smem_doubles * sizeof(double);
+    k_coop<0><<<(unsigned)grid, threads, smem, (cudaStream_t)stream>>>(a, g, d.scratch);
+    if(cudaGetLastError() != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    return (int)ntask;
+}
