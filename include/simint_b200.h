@@ -114,6 +114,18 @@ int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, i
  * sums[2k+1] = sum of absolute values.  Waits for the stream. */
 int simint_b200_basis_checksums(simint_b200_basis * b, double * sums);
 
+/* Autotuner: for every class of the sweep time each kernel variant (the
+ * register kernel where one exists, the cooperative kernel with 1, 2 or 4
+ * primitive quartets per wavefront pass) on the sweep's own tasks and keep
+ * the fastest for `prec`.  Choices are process-wide and are written to the
+ * JSON file $SIMINT_B200_TUNE_FILE when set (read back by simint_init). */
+int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
+                               long long dev_out_doubles, void * stream);
+
+/* The kernel variant chosen for a requested class (0 = untuned default,
+ * 1 = register kernel, 20+B = cooperative kernel with batch B). */
+int simint_b200_variant(const int am[4], int deriv, int prec);
+
 /* Device time of each class in one (non-graph) sweep, milliseconds. */
 int simint_b200_basis_class_times(simint_b200_basis * b, int prec, double * dev_out,
                                   long long dev_out_doubles, void * stream, float * ms);

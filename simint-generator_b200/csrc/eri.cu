@@ -32,6 +32,7 @@
 #include "gen/boys_grid.inc"
 
 namespace sb200 {
+void load_tune_file();
 
 static std::mutex g_mutex;
 static bool g_initialised = false;
@@ -200,6 +201,7 @@ void init_tables()
         const auto & e = g_table.list[k];
         g_unique[{e.am[0], e.am[1], e.am[2], e.am[3]}] = (int)k;
     }
+    load_tune_file();
     const char * o = getenv("SIMINT_B200_ORDERING");
     if(o && (!strcmp(o, "gamess") || !strcmp(o, "GAMESS") || !strcmp(o, "1")))
         g_ordering = SIMINT_B200_ORDERING_GAMESS;
@@ -460,25 +462,35 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
     const UniqueMap u = unique_of(req);
     a.swapB = u.swapB; a.swapK = u.swapK; a.pq = u.pq;
     a.boys = boys_table();
-    if(deriv == 0)
+    const ClassKernels * k = deriv == 0 ? find_kernels(u) : nullptr;
+    int v = variant_of(req, deriv, prec);
+    if(v == VAR_DEFAULT)
+        // untuned default: the register kernel while its contracted tops fit
+        // registers (above ~200 accumulators it spills), else cooperative
+        v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
+    if(v == VAR_STRAIGHT && k)
     {
-        const ClassKernels * k = find_kernels(u);
-        if(k)
+        a.oidx = oidx_table(req, u, ordering());
+        if(!a.oidx)
         {
-            a.oidx = oidx_table(req, u, ordering());
-            if(!a.oidx)
-            {
-                set_error("cannot allocate output index table");
-                return SIMINT_B200_ERR_CUDA;
-            }
-            const int threads = 128;
-            const long long blocks = (a.ntask + threads - 1) / threads;
-            KernFn fn = k->fn[mode][prec == SIMINT_B200_PREC_MIXED ? 1 : 0];
-            fn<<<(unsigned)blocks, threads, 0, stream>>>(a);
-            count_launch(1);
-            return 0;
+            set_error("cannot allocate output index table");
+            return SIMINT_B200_ERR_CUDA;
         }
+        const int threads = 128;
+        const long long blocks = (a.ntask + threads - 1) / threads;
+        KernFn fn = k->fn[mode][prec == SIMINT_B200_PREC_MIXED ? 1 : 0];
+        fn<<<(unsigned)blocks, threads, 0, stream>>>(a);
+        count_launch(1);
+        return 0;
     }
+    if(v >= 20 && coop2_supported(req, deriv, v - 20))
+        return launch_coop2(a, req, deriv, mode, prec, stream, v - 20);
+    if(v == VAR_COOP1 && coop_supported(req, deriv))
+        return launch_coop(a, req, deriv, mode, stream);
+    if(v == VAR_GENERIC)
+        return launch_generic(a, req, u, deriv, mode, stream);
+    if(coop2_supported(req, deriv))
+        return launch_coop2(a, req, deriv, mode, prec, stream);
     if(coop_supported(req, deriv))
         return launch_coop(a, req, deriv, mode, stream);
     return launch_generic(a, req, u, deriv, mode, stream);
@@ -616,3 +628,69 @@ extern "C" long long simint_b200_count_primq(struct simint_multi_shellpair const
         }
     return n;
 }
+
+namespace sb200 {
+
+static std::mutex g_var_mutex;
+static std::map<std::array<int, 6>, int> g_variant;
+
+int variant_of(const int req[4], int deriv, int prec)
+{
+    std::lock_guard<std::mutex> lk(g_var_mutex);
+    auto it = g_variant.find({req[0], req[1], req[2], req[3], deriv, prec});
+    return it == g_variant.end() ? VAR_DEFAULT : it->second;
+}
+
+void set_variant(const int req[4], int deriv, int prec, int v)
+{
+    std::lock_guard<std::mutex> lk(g_var_mutex);
+    g_variant[{req[0], req[1], req[2], req[3], deriv, prec}] = v;
+}
+
+bool has_straight(const int req[4])
+{
+    return find_kernels(unique_of(req)) != nullptr;
+}
+
+// Tuning cache: a small JSON object {"a,b,c,d,deriv,prec": variant, ...}
+// at $SIMINT_B200_TUNE_FILE, read at simint_init and written by the
+// autotuner.
+void load_tune_file()
+{
+    const char * f = getenv("SIMINT_B200_TUNE_FILE");
+    if(!f)
+        return;
+    FILE * fp = fopen(f, "r");
+    if(!fp)
+        return;
+    char line[256];
+    while(fgets(line, sizeof(line), fp))
+    {
+        int q[6], v;
+        if(sscanf(line, " \"%d,%d,%d,%d,%d,%d\": %d", &q[0], &q[1], &q[2], &q[3], &q[4], &q[5], &v) == 7)
+            set_variant(q, q[4], q[5], v);
+    }
+    fclose(fp);
+}
+
+void save_tune_file()
+{
+    const char * f = getenv("SIMINT_B200_TUNE_FILE");
+    if(!f)
+        return;
+    FILE * fp = fopen(f, "w");
+    if(!fp)
+        return;
+    std::lock_guard<std::mutex> lk(g_var_mutex);
+    fprintf(fp, "{\n");
+    size_t n = 0;
+    for(auto & e : g_variant)
+    {
+        fprintf(fp, "  \"%d,%d,%d,%d,%d,%d\": %d%s\n", e.first[0], e.first[1], e.first[2], e.first[3],
+                e.first[4], e.first[5], e.second, ++n < g_variant.size() ? "," : "");
+    }
+    fprintf(fp, "}\n");
+    fclose(fp);
+}
+
+} // namespace sb200

@@ -81,6 +81,18 @@ int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deri
 
 int ncart_of(int l);
 bool coop_supported(const int am[4], int deriv);
+bool coop2_supported(const int am[4], int deriv, int forceB = 0);
+int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
+                 int forceB = 0);
+
+// Kernel variant per (requested class, deriv, precision), chosen by the
+// autotuner: 0 default rule, 1 straight-line, 2 cooperative v2 (20+B: with
+// batch B), 3 cooperative v1, 4 generic.
+enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4 };
+int variant_of(const int req[4], int deriv, int prec);
+void set_variant(const int req[4], int deriv, int prec, int v);
+bool has_straight(const int req[4]);
+void save_tune_file();
 int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_t stream);
 int pair_diag_max(const PairSetDev & dP, int am1, int am2, int n, double * dmax, cudaStream_t stream);
 

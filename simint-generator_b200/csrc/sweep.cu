@@ -500,44 +500,126 @@ extern "C" int simint_b200_basis_quartet(simint_b200_basis const * b, int k, lon
     return 0;
 }
 
+// Issue the launches of class k (ERI chunks + checksums) on `stream`.
+static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout, long long cap,
+                       cudaStream_t stream)
+{
+    int nl = 0;
+    const bool full = cap >= b->total_out;
+    double * dsums = (double *)b->dsums.ptr;
+    QClass & q = b->qcs[k];
+    const long long chunk = full ? q.ntask : std::max<long long>(1, cap / q.nout);
+    for(long long t0 = 0; t0 < q.ntask; t0 += chunk)
+    {
+        const long long cn = std::min(chunk, q.ntask - t0);
+        KernArgs a;
+        fill_args(b, q, a);
+        a.ntask = cn;
+        a.task0 = t0;
+        a.out = full ? dout + q.offset + t0 * q.nout : dout;
+        a.gate = gate();
+        int rc = launch_class(a, q.req, 0, 2, prec, stream);
+        if(rc != 0)
+            return rc;
+        nl++;
+        const long long n = cn * q.nout;
+        const unsigned blocks = (unsigned)std::min<long long>(148 * 8, (n + 255) / 256);
+        k_checksum<<<blocks, 256, 0, stream>>>(a.out, n, dsums + 2 * k);
+        count_launch(1);
+        nl++;
+    }
+    return nl;
+}
+
 // Issue every launch of one sweep on `stream`.  events: optional per-class
 // start/stop pairs (eager runs only).
 static int issue_sweep(simint_b200_basis * b, int prec, double * dout, long long cap,
                        cudaStream_t stream, cudaEvent_t * events)
 {
     int nl = 0;
-    const bool full = cap >= b->total_out;
-    double * dsums = (double *)b->dsums.ptr;
-    cudaMemsetAsync(dsums, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
     for(size_t k = 0; k < b->qcs.size(); k++)
     {
-        QClass & q = b->qcs[k];
         if(events)
             cudaEventRecord(events[2 * k], stream);
-        const long long chunk = full ? q.ntask : std::max<long long>(1, cap / q.nout);
-        for(long long t0 = 0; t0 < q.ntask; t0 += chunk)
-        {
-            const long long cn = std::min(chunk, q.ntask - t0);
-            KernArgs a;
-            fill_args(b, q, a);
-            a.ntask = cn;
-            a.task0 = t0;
-            a.out = full ? dout + q.offset + t0 * q.nout : dout;
-            a.gate = gate();
-            int rc = launch_class(a, q.req, 0, 2, prec, stream);
-            if(rc != 0)
-                return rc;
-            nl++;
-            const long long n = cn * q.nout;
-            const unsigned blocks = (unsigned)std::min<long long>(148 * 8, (n + 255) / 256);
-            k_checksum<<<blocks, 256, 0, stream>>>(a.out, n, dsums + 2 * k);
-            count_launch(1);
-            nl++;
-        }
+        const int r = issue_class(b, k, prec, dout, cap, stream);
+        if(r < 0)
+            return r;
+        nl += r;
         if(events)
             cudaEventRecord(events[2 * k + 1], stream);
     }
     return nl;
+}
+
+extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
+                                          long long dev_out_doubles, void * stream_)
+{
+    if(!b || !dev_out || dev_out_doubles <= 0)
+        return SIMINT_B200_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    for(auto & g : b->graphs)
+        cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+    b->eager_done.clear();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        QClass & q = b->qcs[k];
+        if(q.ntask == 0)
+            continue;
+        std::vector<int> cand;
+        if(has_straight(q.req))
+            cand.push_back(VAR_STRAIGHT);
+        for(int B : {1, 2, 4})
+            if(coop2_supported(q.req, 0, B))
+                cand.push_back(20 + B);
+        if(cand.empty())
+            continue;
+        int best = cand[0];
+        float bestms = 1e30f;
+        for(int v : cand)
+        {
+            set_variant(q.req, 0, prec, v);
+            if(issue_class(b, k, prec, dev_out, dev_out_doubles, stream) < 0)
+                continue;
+            float ms = 1e30f;
+            for(int rep = 0; rep < 2; rep++)
+            {
+                cudaEventRecord(e0, stream);
+                issue_class(b, k, prec, dev_out, dev_out_doubles, stream);
+                cudaEventRecord(e1, stream);
+                cudaEventSynchronize(e1);
+                float t = 0;
+                cudaEventElapsedTime(&t, e0, e1);
+                ms = std::min(ms, t);
+            }
+            if(ms < bestms)
+            {
+                bestms = ms;
+                best = v;
+            }
+        }
+        set_variant(q.req, 0, prec, best);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    save_tune_file();
+    const cudaError_t e = cudaStreamSynchronize(stream);
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("autotune: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    return 0;
+}
+
+extern "C" int simint_b200_variant(const int am[4], int deriv, int prec)
+{
+    return variant_of(am, deriv, prec);
 }
 
 extern "C" int simint_b200_basis_compute(simint_b200_basis * b, int prec, double * dev_out,

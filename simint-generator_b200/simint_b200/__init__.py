@@ -223,6 +223,17 @@ class Basis:
             raise RuntimeError("simint_b200_basis_compute failed (%d): %s" % (r, last_error()))
         return r
 
+    def autotune(self, prec, dev_ptr, ndoubles, stream=0):
+        L = self.lib
+        L.simint_b200_basis_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong, C.c_void_p]
+        r = L.simint_b200_basis_autotune(self.h, prec, C.c_void_p(dev_ptr), ndoubles, C.c_void_p(stream))
+        if r != 0:
+            raise RuntimeError("autotune failed: " + last_error())
+
+    def variant(self, am, prec, deriv=0):
+        self.lib.simint_b200_variant.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int]
+        return self.lib.simint_b200_variant((C.c_int * 4)(*am), deriv, prec)
+
     def checksums(self):
         n = self.lib.simint_b200_basis_nclass(self.h)
         s = np.zeros(2 * max(n, 1))
