@@ -149,18 +149,8 @@ def e2e_rows(sb, lib, S, B, stride, rank=0):
 
 
 def flops_of_class(am, nprimq, nquart):
-    """Algorithmic FLOPs (minimal recurrence plan; FMA = 2): per primitive
-    quartet set-up + Boys + VRR + contraction adds + 3 div + 1 sqrt, per
-    shell quartet the HRR."""
-    from simint_b200.gen.emit import unique_class
-    from simint_b200.gen.plan import class_plan
-    u = unique_class(am)[0]
-    p = class_plan(*u)
-    L = p.L
-    boys = 16 * (L + 1) if L < 4 else 16 + 3 * L + 20
-    setup = 30 + (L + 1)
-    per_prim = setup + boys + p.vrr_flops() + p.ntop() + 4
-    return nprimq * per_prim + nquart * p.hrr_flops()
+    from simint_b200.perfmodel import class_flops
+    return class_flops(am, nprimq, nquart)
 
 
 # ----------------------------------------------------------------------------
@@ -279,6 +269,7 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
         ms = []
+        torch.cuda.nvtx.range_push("timed_" + ("mixed" if prec == sb.MIXED else "fp64"))
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
                 flush.zero_()
@@ -289,6 +280,7 @@ def run_b200(args):
                 e1.record(stream)
                 ms.append((e0, e1))
             torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()

@@ -126,6 +126,12 @@ int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out
  * 1 = register kernel, 20+B = cooperative kernel with batch B). */
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
+/* Pin the kernel variant of a requested class (same codes, plus 3 = first
+ * cooperative kernel and 4 = generic kernel; 0 restores the default rule).
+ * Returns SIMINT_B200_ERR_ARG when the variant does not exist for the class.
+ * Sweep graphs captured earlier are rebuilt on their next use. */
+int simint_b200_set_variant(const int am[4], int deriv, int prec, int variant);
+
 /* Device time of each class in one (non-graph) sweep, milliseconds. */
 int simint_b200_basis_class_times(simint_b200_basis * b, int prec, double * dev_out,
                                   long long dev_out_doubles, void * stream, float * ms);
@@ -200,6 +206,22 @@ int simint_b200_compute_eri_noalloc(int deriv,
                                     struct simint_multi_shellpair const * P, const void * dev_P,
                                     struct simint_multi_shellpair const * Q, const void * dev_Q,
                                     double screen_tol, double * dev_integrals, void * stream);
+
+/* Device-resident form of simint_compute_eri_deriv (no reference
+ * counterpart; its host form is simint_compute_eri_deriv,
+ * skel/simint/ostei/ostei.c:10-41): dev_P and dev_Q hold the packed pair
+ * layout of simint_b200_pack in device memory, dev_integrals receives the
+ * same values simint_compute_eri_deriv(deriv, P, Q, ...) returns, on
+ * `stream`, asynchronously, with the kernel variant, precision and ordering
+ * in force.  Kets are processed in the order of Q.  Working memory is the
+ * calling host thread's (allocated on first need, growth synchronises the
+ * device): calls of one host thread must stay on one stream.  Returns the
+ * shell-quartet count, -1 when the pair-level test screens everything, or a
+ * negative SIMINT_B200_ERR_*. */
+int simint_b200_compute_eri_device(int deriv,
+                                   struct simint_multi_shellpair const * P, const void * dev_P,
+                                   struct simint_multi_shellpair const * Q, const void * dev_Q,
+                                   double screen_tol, double * dev_integrals, void * stream);
 
 #ifdef __cplusplus
 }

@@ -223,7 +223,11 @@ bool DevBuf::reserve(size_t n)
     if(n <= cap)
         return true;
     if(ptr)
+    {
+        // kernels queued by asynchronous entry points may still use it
+        cudaDeviceSynchronize();
         cudaFree(ptr);
+    }
     ptr = nullptr;
     cap = 0;
     size_t want = std::max(n, (size_t)4096);
@@ -413,6 +417,8 @@ extern "C" int simint_b200_set_ordering(int o)
 {
     if(o != SIMINT_B200_ORDERING_PSI4 && o != SIMINT_B200_ORDERING_GAMESS)
         return SIMINT_B200_ERR_ARG;
+    if(g_ordering != o)
+        sb200::bump_settings_epoch();
     g_ordering = o;
     return 0;
 }
@@ -423,6 +429,8 @@ extern "C" int simint_b200_set_precision(int mode, double gate)
 {
     if(mode != SIMINT_B200_PREC_FP64 && mode != SIMINT_B200_PREC_MIXED)
         return SIMINT_B200_ERR_ARG;
+    if(g_precision != mode || g_gate != gate)
+        sb200::bump_settings_epoch();
     g_precision = mode;
     g_gate = gate;
     return 0;
@@ -593,6 +601,88 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     return (int)nquart;
 }
 
+namespace sb200 {
+
+// Identity ket order per device for the device-resident entry point; grown
+// (never shrunk) under a lock, so kernels already queued keep a valid
+// buffer until the device is synchronised before a regrowth.
+static const int * identity_kord(long long n)
+{
+    static std::mutex m;
+    static std::map<int, std::pair<int *, long long>> bufs;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(m);
+    auto & b = bufs[dev];
+    if(b.second >= n)
+        return b.first;
+    long long cap = std::max<long long>(n, 1 << 16);
+    std::vector<int> h(cap);
+    for(long long k = 0; k < cap; k++)
+        h[k] = (int)k;
+    if(b.first)
+    {
+        cudaDeviceSynchronize();
+        cudaFree(b.first);
+        b = {nullptr, 0};
+    }
+    int * d = nullptr;
+    if(cudaMalloc(&d, cap * sizeof(int)) != cudaSuccess)
+        return nullptr;
+    if(cudaMemcpy(d, h.data(), cap * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    {
+        cudaFree(d);
+        return nullptr;
+    }
+    b = {d, cap};
+    return d;
+}
+
+} // namespace sb200
+
+extern "C" int simint_b200_compute_eri_device(int deriv,
+                                              struct simint_multi_shellpair const * P, const void * dev_P,
+                                              struct simint_multi_shellpair const * Q, const void * dev_Q,
+                                              double screen_tol, double * dev_integrals, void * stream)
+{
+    if(!P || !Q || !dev_P || !dev_Q || !dev_integrals || deriv < 0 || deriv > SIMINT_OSTEI_MAXDER)
+    {
+        set_error("bad argument to simint_b200_compute_eri_device");
+        return SIMINT_B200_ERR_ARG;
+    }
+    const double tol2 = screen_tol * screen_tol;
+    if(screen_tol > 0.0 && (P->screen_max * Q->screen_max) < tol2)
+        return -1;
+    init_tables();
+    if(ensure_device() < 0)
+        return SIMINT_B200_ERR_NODEVICE;
+    const long long nquart = (long long)P->nshell12_clip * Q->nshell12_clip;
+    if(nquart == 0)
+        return 0;
+    const int * kord = identity_kord(Q->nshell12_clip);
+    if(!kord)
+    {
+        set_error("cannot allocate the ket order");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    PackedLayout LP, LQ;
+    pack_pairs(P, nullptr, LP);
+    pack_pairs(Q, nullptr, LQ);
+    const PairSetDev dP = device_view((const char *)dev_P, LP, P->screen_max);
+    const PairSetDev dQ = device_view((const char *)dev_Q, LQ, Q->screen_max);
+    int r = launch_rectangle(P, dP, Q, dQ, kord, screen_tol, deriv, precision(), gate(),
+                             dev_integrals, (cudaStream_t)stream);
+    if(r < 0)
+        return r;
+    cudaError_t e = cudaGetLastError();
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    return (int)nquart;
+}
+
 extern "C" int simint_compute_eri(struct simint_multi_shellpair const * P,
                                   struct simint_multi_shellpair const * Q,
                                   double screen_tol, double * work, double * integrals)
@@ -633,6 +723,10 @@ namespace sb200 {
 
 static std::mutex g_var_mutex;
 static std::map<std::array<int, 6>, int> g_variant;
+static std::atomic<long long> g_settings_epoch{0};
+
+long long settings_epoch() { return g_settings_epoch.load(); }
+void bump_settings_epoch() { g_settings_epoch++; }
 
 int variant_of(const int req[4], int deriv, int prec)
 {
@@ -645,6 +739,7 @@ void set_variant(const int req[4], int deriv, int prec, int v)
 {
     std::lock_guard<std::mutex> lk(g_var_mutex);
     g_variant[{req[0], req[1], req[2], req[3], deriv, prec}] = v;
+    g_settings_epoch++;
 }
 
 bool has_straight(const int req[4])
@@ -694,3 +789,42 @@ void save_tune_file()
 }
 
 } // namespace sb200
+
+extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int variant)
+{
+    using namespace sb200;
+    if(!am || (deriv != 0 && deriv != 1) ||
+       (prec != SIMINT_B200_PREC_FP64 && prec != SIMINT_B200_PREC_MIXED))
+        return SIMINT_B200_ERR_ARG;
+    for(int k = 0; k < 4; k++)
+        if(am[k] < 0 || am[k] > SIMINT_OSTEI_MAXAM)
+            return SIMINT_B200_ERR_CLASS;
+    bool ok = false;
+    switch(variant)
+    {
+        case VAR_DEFAULT:
+        case VAR_GENERIC:
+            ok = true;
+            break;
+        case VAR_STRAIGHT:
+            ok = deriv == 0 && has_straight(am);
+            break;
+        case VAR_COOP1:
+            ok = coop_supported(am, deriv);
+            break;
+        case 21:
+        case 22:
+        case 24:
+            ok = coop2_supported(am, deriv, variant - 20);
+            break;
+        default:
+            ok = false;
+    }
+    if(!ok)
+    {
+        set_error("kernel variant not available for this class");
+        return SIMINT_B200_ERR_ARG;
+    }
+    set_variant(am, deriv, prec, variant);
+    return 0;
+}

@@ -91,6 +91,10 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4 };
 int variant_of(const int req[4], int deriv, int prec);
 void set_variant(const int req[4], int deriv, int prec, int v);
+// Incremented whenever a setting that captured sweep graphs bake in changes
+// (kernel variant, ordering, precision gate); graphs older than it are rebuilt.
+long long settings_epoch();
+void bump_settings_epoch();
 bool has_straight(const int req[4]);
 void save_tune_file();
 int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_t stream);

@@ -124,6 +124,7 @@ struct simint_b200_basis
     DevBuf dsums;
     std::map<std::array<long long, 3>, cudaGraphExec_t> graphs;
     std::map<std::array<long long, 3>, int> eager_done;
+    long long graph_epoch = -1;            // settings_epoch() the graphs were built under
     cudaStream_t own_stream = nullptr;
     int nlaunch = 0;
 };
@@ -628,6 +629,17 @@ extern "C" int simint_b200_basis_compute(simint_b200_basis * b, int prec, double
     if(!b || !dev_out || dev_out_doubles <= 0)
         return SIMINT_B200_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
+    if(b->graph_epoch != settings_epoch())
+    {
+        // a kernel variant, the ordering or the precision gate changed:
+        // graphs captured before bake in the old choice
+        cudaStreamSynchronize(stream);
+        for(auto & g : b->graphs)
+            cudaGraphExecDestroy(g.second);
+        b->graphs.clear();
+        b->eager_done.clear();
+        b->graph_epoch = settings_epoch();
+    }
     const std::array<long long, 3> key = {prec, (long long)(uintptr_t)dev_out, dev_out_doubles};
     auto it = b->graphs.find(key);
     if(it != b->graphs.end())

@@ -109,6 +109,25 @@ def compute_eri(P, Q, screen_tol=0.0, deriv=0, lib=None):
     return r, out
 
 
+VAR_DEFAULT, VAR_STRAIGHT, VAR_COOP1, VAR_GENERIC = 0, 1, 3, 4
+VAR_COOP2 = {1: 21, 2: 22, 4: 24}
+
+
+def get_variant(am, deriv=0, prec=0, lib=None):
+    """Kernel variant in force for a requested class (simint_b200_variant)."""
+    lib = lib or load()
+    lib.simint_b200_variant.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int]
+    return lib.simint_b200_variant((C.c_int * 4)(*am), deriv, prec)
+
+
+def set_variant(am, variant, deriv=0, prec=0, lib=None):
+    """Pin the kernel variant of a requested class; returns the C status
+    (0, or SIMINT_B200_ERR_ARG when the variant does not exist for it)."""
+    lib = lib or load()
+    lib.simint_b200_set_variant.argtypes = [C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int]
+    return lib.simint_b200_set_variant((C.c_int * 4)(*am), deriv, prec, variant)
+
+
 class Basis:
     """simint_b200_basis: a device-resident, Schwarz-screened sweep."""
 

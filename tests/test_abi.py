@@ -56,3 +56,21 @@ def test_worksize_matches_reference_generator():
     assert lib.simint_eri_worksize(0, 1) == exp_l1
     assert lib.simint_eri_workmem(0, 1) == 8 * exp_l1
     assert lib.simint_eri_worksize(1, 2) == ((16 * 5386 + 7) & ~7) + ((37116 + 7) & ~7) + 8 * 5801
+
+
+def test_set_variant_validates_without_a_device():
+    """simint_b200_set_variant accepts only variants that exist for a class
+    (host-side planning; no kernel runs)."""
+    lib = sb.load()
+    lib.simint_init()
+    am = (2, 2, 2, 2)
+    assert sb.set_variant(am, 24, 0, sb.FP64, lib) == 0
+    assert sb.get_variant(am, 0, sb.FP64, lib) == 24
+    assert sb.get_variant(am, 0, sb.MIXED, lib) == 0          # per precision
+    assert sb.set_variant(am, 23, 0, sb.FP64, lib) != 0       # no batch-3 kernel
+    assert sb.set_variant(am, 99, 0, sb.FP64, lib) != 0
+    assert sb.set_variant((5, 0, 0, 0), 4, 0, sb.FP64, lib) != 0
+    assert sb.set_variant((4, 4, 4, 4), 1, 0, sb.FP64, lib) != 0   # no register kernel
+    assert sb.set_variant((1, 1, 1, 1), 1, 1, sb.FP64, lib) != 0   # register kernels: deriv 0 only
+    assert sb.set_variant(am, 0, 0, sb.FP64, lib) == 0
+    assert sb.get_variant(am, 0, sb.FP64, lib) == 0

@@ -1,0 +1,73 @@
+"""GPU: every kernel variant of a class against the CPU oracle.
+
+The autotuner may pick, per class, the register kernel, the cooperative
+kernel with 1, 2 or 4 primitive quartets per wavefront pass, the first
+cooperative kernel or the generic kernel; each must meet the FP64 parity bar
+on its own.  Variants are pinned with simint_b200_set_variant and restored
+to the default rule afterwards.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import simint_b200 as sb
+from simint_b200.capi import ShellSet
+from oracle import load_oracle
+from _util import class_shells, oracle_pairs, oracle_eri, parity_bad
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [sb.VAR_STRAIGHT, 21, 22, 24, sb.VAR_COOP1, sb.VAR_GENERIC]
+CLASSES = [(0, 0, 0, 0), (1, 0, 1, 0), (1, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 1), (2, 2, 2, 2),
+           (3, 1, 2, 1), (3, 2, 1, 0), (2, 3, 3, 0), (3, 3, 2, 2), (4, 2, 1, 1), (3, 3, 3, 3)]
+
+
+@pytest.fixture(scope="module")
+def libs():
+    lib = sb.load()
+    lib.simint_init()
+    lib.simint_b200_set_ordering(0)
+    return lib, load_oracle()
+
+
+def _case(lib, orc, am, deriv, seed):
+    rng = np.random.default_rng(seed)
+    big = sum(am) >= 9
+    shells, grp = class_shells(rng, am, nsh=(1, 1, 1, 1) if big else (2, 1, 2, 1),
+                               nprim=(1, 2) if big else (1, 3))
+    S = ShellSet(shells)
+    orc.oracle_normalize_shells(S.n, S.ptr(0))
+    bra = [(i, j) for i in grp[0] for j in grp[1]]
+    ket = [(i, j) for i in grp[2] for j in grp[3]]
+    oP, oQ = oracle_pairs(orc, S, bra), oracle_pairs(orc, S, ket)
+    rr, ref = oracle_eri(orc, oP, oQ, 0.0, deriv, 0)
+    orc.oracle_free_pair(C.byref(oP))
+    orc.oracle_free_pair(C.byref(oQ))
+    return S, bra, ket, rr, ref
+
+
+@pytest.mark.parametrize("deriv", [0, 1])
+@pytest.mark.parametrize("am", CLASSES, ids=lambda a: "".join("spdfg"[x] for x in a))
+def test_every_variant_matches_oracle(libs, am, deriv):
+    lib, orc = libs
+    if deriv and sum(am) > 8:
+        pytest.skip("deriv=1 sampled up to l_total 8 here")
+    S, bra, ket, rr, ref = _case(lib, orc, am, deriv, 4242 + 13 * sum(am) + am[0] + deriv)
+    P = sb.make_pairs(lib, S, bra)
+    Q = sb.make_pairs(lib, S, ket)
+    ran = []
+    try:
+        for v in VARIANTS:
+            if sb.set_variant(am, v, deriv, sb.FP64, lib) != 0:
+                continue
+            ran.append(v)
+            r, out = sb.compute_eri(P, Q, 0.0, deriv, lib)
+            assert r == rr, (v, r, rr)
+            bad, dmax = parity_bad(out, ref)
+            assert len(bad) == 0, (v, dmax)
+    finally:
+        sb.set_variant(am, sb.VAR_DEFAULT, deriv, sb.FP64, lib)
+        lib.simint_free_multi_shellpair(C.byref(P))
+        lib.simint_free_multi_shellpair(C.byref(Q))
+    assert sb.VAR_GENERIC in ran and len(ran) >= 2, ran
