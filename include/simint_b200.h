@@ -115,15 +115,17 @@ int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, i
 int simint_b200_basis_checksums(simint_b200_basis * b, double * sums);
 
 /* Autotuner: for every class of the sweep time each kernel variant (the
- * register kernel where one exists, the cooperative kernel with 1, 2 or 4
- * primitive quartets per wavefront pass) on the sweep's own tasks and keep
+ * register kernel where one exists, the cooperative kernel with 256 or 128
+ * threads and 1, 2 or 4 primitive quartets per wavefront pass) on the
+ * sweep's own tasks and keep
  * the fastest for `prec`.  Choices are process-wide and are written to the
  * JSON file $SIMINT_B200_TUNE_FILE when set (read back by simint_init). */
 int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
                                long long dev_out_doubles, void * stream);
 
 /* The kernel variant chosen for a requested class (0 = untuned default,
- * 1 = register kernel, 20+B = cooperative kernel with batch B). */
+ * 1 = register kernel, 20+B / 40+B = cooperative kernel with 256 / 128
+ * threads and batch B = 1, 2, 4). */
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first

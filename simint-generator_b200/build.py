@@ -82,8 +82,11 @@ def build(max_am=4, limit=DEFAULT_LIMIT, jobs=None, verbose=False, only=None):
         objs.append(obj)
         work.append((s, obj))
     logs = []
+    # generated kernels include only the device header and the kernel table
+    gen_headers = [os.path.join(CSRC, "ostei_device.cuh"), os.path.join(CSRC, "kernels.h")]
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        futs = [ex.submit(_compile, s, o, headers, verbose) for s, o in work]
+        futs = [ex.submit(_compile, s, o, gen_headers if os.path.dirname(s) == GEN else headers, verbose)
+                for s, o in work]
         for f in futs:
             src, dt, err = f.result()
             if dt > 0:

@@ -1,4 +1,4 @@
-// CTA-cooperative ERI kernel, table-driven (v2): large AM classes, deriv 0/1.
+// CTA-cooperative ERI kernel, table-driven: large AM classes, deriv 0/1.
 //
 // One CTA computes one shell quartet at a time.  Per class the host builds
 // (once) a table of work items: one item per Cartesian pair (e-cart, f-cart)
@@ -8,17 +8,26 @@
 // centre order OSTEI_VRR_Algorithm_Base.cpp:449-469).  Blocks are grouped
 // into anti-diagonal wavefronts s = e+f (a block depends only on s-1 and
 // s-2) and each block keeps only the auxiliary orders m it really feeds.
+// Inside a wavefront the items are sorted by shape (m count, which sources
+// exist) so the threads of a warp take the same branches.
 //
 // Surviving primitive quartets (the reference's screening tests) are
-// compacted in order and processed B at a time: a thread owns an item and
-// runs it for all B primitive quartets and all its m values, so one
-// __syncthreads per wavefront serves B primitive quartets and every thread
-// has B*m independent FMA chains.  Top quartets are summed into per-tag
-// accumulators by the owning thread (deriv weights of
-// OSTEIDeriv1_Writer.cpp:53-94).  After the primitive loop the HRR
-// (OSTEI_HRR_Algorithm_Base.cpp:160-283) runs level by level over all
-// columns (bra side) and rows (ket side) in shared memory; deriv=1 components
-// are formed by translational invariance (OSTEIDeriv1_Writer.cpp:334-537).
+// compacted in order; their set-up and Boys values are computed 16 at a time
+// by 16 threads into shared memory, then processed B at a time: a thread
+// owns an item and runs it for all B primitive quartets and all its m
+// values, so one __syncthreads per wavefront serves B primitive quartets.
+// Per primitive quartet the step coefficients are stored as six
+// (direction, side) combos of [X, Y, Z, 1/2s] so an item reads its four
+// coefficients with two 16-byte loads.  Top quartets are summed into
+// per-tag accumulators by the owning thread in primitive order (deriv
+// weights of OSTEIDeriv1_Writer.cpp:53-94).  After the primitive loop the
+// HRR (OSTEI_HRR_Algorithm_Base.cpp:160-283) runs level by level in shared
+// memory: the first layer reads the accumulators, the last layer writes its
+// destination directly; deriv=1 components are formed by translational
+// invariance (OSTEIDeriv1_Writer.cpp:334-537).
+//
+// Variants: 256 or 128 threads per CTA, B = 1, 2 or 4 (variant codes
+// 20+B and 40+B).
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -36,8 +45,19 @@
 
 #define C2_MAXL 10
 #define C2_MAXS 20
-#define C2_NCOEF 24
-#define C2_THREADS 256
+#define C2_NCOEF 32          // per primitive quartet: 6 combos x 4, 1/2(p+q), 4 deriv weights, pad
+#define C2_SETUP 16          // primitive quartets set up in parallel
+#define C2_MAXN 225          // Cartesian pairs of (g g)
+
+enum { K_O2PQ = 24, K_W1 = 25 };
+
+struct C2Item
+{
+    int4 a;                  // dst, src1, src2, src3 (offsets of the m = 0 slot; -1 = none)
+    int4 b;                  // combo | mlen << 4 | has2 << 9 | has3 << 10,  acc index of tag 0 (-1 = none),
+                             // mask of tags >= 1,  gE | gF << 16
+    double2 c;               // nA, nB (integer factors of the 1/2p and 1/2(p+q) terms)
+};
 
 struct C2Params
 {
@@ -51,18 +71,15 @@ struct C2Params
     int wsize;                    // doubles per (wave, batch entry)
     int smax;                     // last wavefront
     int wstart[C2_MAXS + 2];      // item range of wavefront s: [wstart[s], wstart[s+1])
-    const int4 * items;           // 2 x int4 per item
-    int off_acc, off_coef, off_surv, off_hrr;   // shared-memory layout (doubles)
+    const C2Item * items;
+    int off_acc, off_prep, off_surv, off_hrr_b, off_hrr_mid;   // shared-memory layout (doubles)
+    int prep_stride;              // doubles per prepared primitive quartet
     int hrr_layer;                // doubles per HRR layer buffer
     int smem_doubles;
     int ordering;
     int res_size;                 // deriv 1: doubles of all target results per CTA
     int res_off[6];
 };
-
-// item layout
-//   a = {dst, src1, src2, src3}                 (offsets of the m = 0 slot)
-//   b = {x | ket << 2 | nA << 3 | nB << 8 | mlen << 16,  gE | gF << 16,  tagmask, 0}
 
 __device__ __forceinline__ int c2_lev_off(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
 __device__ __forceinline__ int c2_nc(int l) { return ((l + 1) * (l + 2)) / 2; }
@@ -82,85 +99,159 @@ __device__ __forceinline__ int c2_index(const CartInfo * __restrict__ ci, int g,
     return c.pos;
 }
 
-// coefficient slots of one primitive quartet in shared memory
-enum { K_XP0, K_XP1, K_XP2, K_XQ0, K_XQ1, K_XQ2, K_AOP0, K_AOP1, K_AOP2, K_AOQ0, K_AOQ1, K_AOQ2,
-       K_AP, K_AQ, K_O2P, K_O2Q, K_O2PQ, K_W1, K_W2, K_W3, K_W4 };
-
 // One side of the HRR for every column at once, layer by layer in shared
 // memory.  in(g, col) gives the tops (functions on the top centre, levels
-// lo..lt); out(r, col, v) receives the (ta tb) block.
-template<typename IN, typename OUT>
+// lo..lt); out(r, col, v) receives the (ta tb) block, r = pa * nc(tb) + pb.
+// Threads form a (row, column) grid so no element needs a division.
+template<int NT, typename IN, typename OUT>
 __device__ void c2_hrr_side(const CartInfo * __restrict__ ci, int right_step, int ta, int tb, int ncol,
                             double X0, double X1, double X2, IN in, OUT out,
-                            double * __restrict__ L0, double * __restrict__ L1)
+                            double * __restrict__ LA, double * __restrict__ LB)
 {
     const int lt = ta + tb;
     const int lo = right_step ? ta : tb;
     const int sl_max = right_step ? tb : ta;
-    const int tid = threadIdx.x, nth = blockDim.x;
-    // layer 0: tops, index (gt - lev_off(lo)) * ncol + col
-    const int n0 = (c2_lev_off(lt + 1) - c2_lev_off(lo)) * ncol;
-    for(int k = tid; k < n0; k += nth)
+    const int nbb = c2_nc(tb);
+    const int tid = threadIdx.x;
+    const int TC = ncol < NT ? ncol : NT;
+    const int TR = NT / TC;
+    const int tc = tid % TC, tr = tid / TC;
+    if(sl_max == 0)
     {
-        const int col = k % ncol, gt = c2_lev_off(lo) + k / ncol;
-        L0[k] = in(gt, col);
+        // nothing to transfer: the tops at level lt are the block
+        const int nr = c2_nc(ta) * nbb;
+        if(tr < TR)
+            for(int r = tr; r < nr; r += TR)
+                for(int col = tc; col < ncol; col += TC)
+                    out(r, col, in(c2_lev_off(lt) + r, col));
+        __syncthreads();
+        return;
     }
-    __syncthreads();
-    double * src = L0;
-    double * dst = L1;
+    double * dst = LA;
+    const double * src = LB;
     for(int sl = 1; sl <= sl_max; sl++)
     {
         // layer sl: (gt in levels lo..lt-sl) x (gs in level sl) x col
         const int ngt = c2_lev_off(lt - sl + 1) - c2_lev_off(lo);
-        const int ngtp = c2_lev_off(lt - sl + 2) - c2_lev_off(lo);   // previous layer's gt range
         const int nsl = c2_nc(sl), nslm = c2_nc(sl - 1);
-        const int n = ngt * nsl * ncol;
-        for(int k = tid; k < n; k += nth)
-        {
-            const int col = k % ncol;
-            const int r = k / ncol;
-            const int ps = r % nsl, it = c2_lev_off(lo) + r / nsl;
-            const int is = c2_lev_off(sl) + ps;
-            const int x = ci[is].dir;
-            const int ism = ci[is].m1[x];
-            const int itp = ci[it].p1[x];
-            const int pm = ci[ism].pos;
-            const double a = src[(((it - c2_lev_off(lo)) * nslm) + pm) * ncol + col];
-            const double b = src[(((itp - c2_lev_off(lo)) * nslm) + pm) * ncol + col];
-            const double X = x == 0 ? X0 : (x == 1 ? X1 : X2);
-            dst[k] = right_step ? fma(X, a, b) : fma(-X, a, b);
-            (void)ngtp;
-        }
+        const int nrow = ngt * nsl;
+        const bool last = sl == sl_max;
+        if(tr < TR)
+            for(int r = tr; r < nrow; r += TR)
+            {
+                const int ps = r % nsl, itq = r / nsl;
+                const int it = c2_lev_off(lo) + itq;
+                const int is = c2_lev_off(sl) + ps;
+                const int x = ci[is].dir;
+                const int ism = ci[is].m1[x];
+                const int itp = ci[it].p1[x];
+                const int pm = ci[ism].pos;
+                double X = x == 0 ? X0 : (x == 1 ? X1 : X2);
+                if(!right_step)
+                    X = -X;
+                // on the last layer gt is at level lo: (pt, ps) -> (pa, pb)
+                const int orow = right_step ? itq * nbb + ps : ps * nbb + itq;
+                if(sl == 1)
+                {
+                    for(int col = tc; col < ncol; col += TC)
+                    {
+                        const double v = fma(X, in(it, col), in(itp, col));
+                        if(last) out(orow, col, v);
+                        else dst[r * ncol + col] = v;
+                    }
+                }
+                else
+                {
+                    const double * sa = src + ((it - c2_lev_off(lo)) * nslm + pm) * ncol;
+                    const double * sb = src + ((itp - c2_lev_off(lo)) * nslm + pm) * ncol;
+                    for(int col = tc; col < ncol; col += TC)
+                    {
+                        const double v = fma(X, sa[col], sb[col]);
+                        if(last) out(orow, col, v);
+                        else dst[r * ncol + col] = v;
+                    }
+                }
+            }
         __syncthreads();
-        double * t = src; src = dst; dst = t;
+        double * t = (double *)src;
+        src = dst;
+        dst = t;
     }
-    // the last layer holds gt at level (right ? ta : tb), gs at level sl_max
-    const int na = c2_nc(ta), nb = c2_nc(tb);
-    const int nsl = c2_nc(sl_max);
-    for(int k = tid; k < na * nb * ncol; k += nth)
-    {
-        const int col = k % ncol, r = k / ncol;
-        const int pa = r / nb, pb = r % nb;
-        const int pt = right_step ? pa : pb, ps = right_step ? pb : pa;
-        out(r, col, src[(pt * nsl + ps) * ncol + col]);
-    }
-    __syncthreads();
 }
 
-template<int MODE, bool MIXED>
-__global__ void __launch_bounds__(C2_THREADS) k_coop2(const KernArgs a, const C2Params p,
-                                                     double * __restrict__ gres)
+// Boys values F_0..F_L(T) times prefac into F (shared memory), the
+// reference's split: L < 4 every order from the Taylor grid (or the
+// asymptotic form for T >= 36.5), L >= 4 F_L then downward recursion
+// (boys.h:14-92, boys_taylor.h:14-39, boys_long.h:14-58).
+__device__ __forceinline__ void c2_boys(const double * __restrict__ tab, double T, int L, double prefac,
+                                        double * __restrict__ F)
 {
-    extern __shared__ double sm[];
+    if(L < 4)
+    {
+        if(T >= 0.0 && T < 36.5)
+        {
+            const int idx = (int)(10.0 * (T + 0.05));
+            const double dx = (double)idx * 0.1 - T;
+            for(int n = 0; n <= L; n++)
+                F[n] = boys_taylor(tab + idx * 32 + n, dx) * prefac;
+        }
+        else
+        {
+            const double x1 = 1.0 / T;
+            double x2 = sqrt(x1);
+            for(int n = 0; n <= L; n++)
+            {
+                F[n] = (__ldg(tab + SB_BOYS_LONGFAC_OFF + n) * x2) * prefac;
+                x2 *= x1;
+            }
+        }
+        return;
+    }
+    double f;
+    if(T >= 0.0 && T < 36.5)
+    {
+        const int idx = (int)(10.0 * (T + 0.05));
+        const double dx = (double)idx * 0.1 - T;
+        f = boys_taylor(tab + idx * 32 + L, dx);
+    }
+    else
+        f = __ldg(tab + SB_BOYS_LONGFAC_OFF + L) * pow(T, -((double)L + 0.5));
+    const double x2 = 2.0 * T;
+    const double ex = exp(-T);
+    F[L] = f * prefac;
+    for(int n = L - 1; n >= 0; n--)
+    {
+        f = (1.0 / (2.0 * n + 1.0)) * fma(x2, f, ex);
+        F[n] = f * prefac;
+    }
+}
+
+template<int MODE, int NT, int DERIV>
+__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs a, const C2Params p,
+                                                                 double * __restrict__ gres)
+{
+    extern __shared__ __align__(16) double sm[];
     __shared__ CartInfo ci[CI_NCART];
     __shared__ int s_cnt;
-    for(int k = threadIdx.x; k < CI_NCART; k += blockDim.x)
+    __shared__ int wcount[NT / 32];
+    __shared__ int obra[C2_MAXN], oket[C2_MAXN];
+    const int tid = threadIdx.x;
+    for(int k = tid; k < CI_NCART; k += NT)
         ci[k] = c_cartinfo[k];
-    const int tid = threadIdx.x, nth = blockDim.x;
-    const int B = p.B, L = p.L, W = p.wsize;
+    __syncthreads();
+    const int * am = p.am;
+    const int n0 = c2_nc(am[0]), n1 = c2_nc(am[1]), n2 = c2_nc(am[2]), n3 = c2_nc(am[3]);
+    // output offsets of the (a b) rows and (c d) columns of the requested class
+    for(int k = tid; k < n0 * n1; k += NT)
+        obra[k] = (c2_index(ci, c2_lev_off(am[0]) + k / n1, p.ordering) * n1
+                   + c2_index(ci, c2_lev_off(am[1]) + k % n1, p.ordering)) * (n2 * n3);
+    for(int k = tid; k < n2 * n3; k += NT)
+        oket[k] = c2_index(ci, c2_lev_off(am[2]) + k / n3, p.ordering) * n3
+                + c2_index(ci, c2_lev_off(am[3]) + k % n3, p.ordering);
+    const int B = p.B, L = p.L, W = p.wsize, PS = p.prep_stride;
     double * wave = sm;
     double * acc = sm + p.off_acc;
-    double * coef = sm + p.off_coef;
+    double * prep = sm + p.off_prep;
     int * surv = (int *)(sm + p.off_surv);
     double * res = gres + (size_t)blockIdx.x * p.res_size;
     __syncthreads();
@@ -172,16 +263,15 @@ __global__ void __launch_bounds__(C2_THREADS) k_coop2(const KernArgs a, const C2
         task_of<MODE>(a, t, iP, iQ, off);
         QuartetCtx c;
         make_ctx(a, iP, iQ, c);
-        for(int k = tid; k < p.acc_size; k += nth)
+        for(int k = tid; k < p.acc_size; k += NT)
             acc[k] = 0.0;
         const int ni = c.bi1 - c.bi0, nj = c.kj1 - c.kj0;
         const int ncand = ni * nj;
-        for(int k0 = 0; k0 < ncand; k0 += nth)
+        for(int k0 = 0; k0 < ncand; k0 += NT)
         {
-            // ordered compaction of the surviving primitive quartets k0..k0+nth
+            // ordered compaction of the surviving primitive quartets k0..k0+NT
             if(tid == 0)
                 s_cnt = 0;
-            __syncthreads();
             const int k = k0 + tid;
             bool ok = false;
             if(k < ncand)
@@ -192,7 +282,6 @@ __global__ void __launch_bounds__(C2_THREADS) k_coop2(const KernArgs a, const C2
             }
             const unsigned ball = __ballot_sync(0xffffffffu, ok);
             const int lane = tid & 31, warp = tid >> 5;
-            __shared__ int wcount[C2_THREADS / 32];
             if(lane == 0)
                 wcount[warp] = __popc(ball);
             __syncthreads();
@@ -201,146 +290,137 @@ __global__ void __launch_bounds__(C2_THREADS) k_coop2(const KernArgs a, const C2
                 base += wcount[w];
             if(ok)
                 surv[base + __popc(ball & ((1u << lane) - 1))] = k;
-            if(tid == nth - 1)
+            if(tid == NT - 1)
             {
                 int tot = 0;
-                for(int w = 0; w < nth / 32; w++)
+                for(int w = 0; w < NT / 32; w++)
                     tot += wcount[w];
                 s_cnt = tot;
             }
             __syncthreads();
             const int nsurv = s_cnt;
-            for(int b0 = 0; b0 < nsurv; b0 += B)
+            for(int g0 = 0; g0 < nsurv; g0 += C2_SETUP)
             {
-                const int nb = min(B, nsurv - b0);
-                // set-up and Boys of the batch: one thread per primitive quartet
-                if(tid < nb)
+                const int ng = min(C2_SETUP, nsurv - g0);
+                // set-up and Boys of up to C2_SETUP primitive quartets in parallel
+                if(tid < ng)
                 {
-                    const int kk = surv[b0 + tid];
+                    const int kk = surv[g0 + tid];
                     const int i = c.bi0 + kk / nj, j = c.kj0 + kk % nj;
                     const BraPrim bp = load_bra_prim(c, i);
                     PrimSetup s;
                     prim_setup(c, bp, j, s);
-                    double * cf = coef + tid * C2_NCOEF;
-                    cf[K_XP0] = p.brastep_j ? s.PAx : s.PBx;
-                    cf[K_XP1] = p.brastep_j ? s.PAy : s.PBy;
-                    cf[K_XP2] = p.brastep_j ? s.PAz : s.PBz;
-                    cf[K_XQ0] = p.ketstep_l ? s.QCx : s.QDx;
-                    cf[K_XQ1] = p.ketstep_l ? s.QCy : s.QDy;
-                    cf[K_XQ2] = p.ketstep_l ? s.QCz : s.QDz;
-                    cf[K_AOP0] = s.aopPQx; cf[K_AOP1] = s.aopPQy; cf[K_AOP2] = s.aopPQz;
-                    cf[K_AOQ0] = s.aoqPQx; cf[K_AOQ1] = s.aoqPQy; cf[K_AOQ2] = s.aoqPQz;
-                    cf[K_AP] = s.a_over_p; cf[K_AQ] = s.a_over_q;
-                    cf[K_O2P] = s.oo2p; cf[K_O2Q] = s.oo2q; cf[K_O2PQ] = s.oo2pq;
-                    cf[K_W1] = s.c2a; cf[K_W2] = s.c2b; cf[K_W3] = s.c2c; cf[K_W4] = s.c2d;
-                    double F[24];
-                    if(L < 4)
+                    double * cf = prep + tid * PS;
+                    const double XP[3] = {p.brastep_j ? s.PAx : s.PBx, p.brastep_j ? s.PAy : s.PBy,
+                                          p.brastep_j ? s.PAz : s.PBz};
+                    const double XQ[3] = {p.ketstep_l ? s.QCx : s.QDx, p.ketstep_l ? s.QCy : s.QDy,
+                                          p.ketstep_l ? s.QCz : s.QDz};
+                    const double YP[3] = {s.aopPQx, s.aopPQy, s.aopPQz};
+                    const double YQ[3] = {s.aoqPQx, s.aoqPQy, s.aoqPQz};
+                    #pragma unroll
+                    for(int x = 0; x < 3; x++)
                     {
-                        if(s.T >= 0.0 && s.T < 36.5)
-                        {
-                            const int idx = (int)(10.0 * (s.T + 0.05));
-                            const double dx = (double)idx * 0.1 - s.T;
-                            for(int n = 0; n <= L; n++)
-                                F[n] = boys_taylor(c.boys + idx * 32 + n, dx);
-                        }
-                        else
-                        {
-                            const double x1 = 1.0 / s.T;
-                            double x2 = sqrt(x1);
-                            for(int n = 0; n <= L; n++)
-                            {
-                                F[n] = c.boys[SB_BOYS_LONGFAC_OFF + n] * x2;
-                                x2 *= x1;
-                            }
-                        }
+                        double * b4 = cf + 4 * x;
+                        b4[0] = XP[x]; b4[1] = YP[x]; b4[2] = s.a_over_p; b4[3] = s.oo2p;
+                        double * k4 = cf + 12 + 4 * x;
+                        k4[0] = XQ[x]; k4[1] = YQ[x]; k4[2] = s.a_over_q; k4[3] = s.oo2q;
                     }
-                    else
-                    {
-                        if(s.T >= 0.0 && s.T < 36.5)
-                        {
-                            const int idx = (int)(10.0 * (s.T + 0.05));
-                            const double dx = (double)idx * 0.1 - s.T;
-                            F[L] = boys_taylor(c.boys + idx * 32 + L, dx);
-                        }
-                        else
-                            F[L] = c.boys[SB_BOYS_LONGFAC_OFF + L] * pow(s.T, -((double)L + 0.5));
-                        const double x2 = 2.0 * s.T;
-                        const double ex = exp(-s.T);
-                        for(int n = L - 1; n >= 0; n--)
-                            F[n] = (1.0 / (2.0 * n + 1.0)) * fma(x2, F[n + 1], ex);
-                    }
-                    double * w0 = wave + tid * W;           // wavefront 0 = block (0,0)
-                    for(int n = 0; n <= L; n++)
-                        w0[n] = F[n] * s.prefac;
+                    cf[K_O2PQ] = s.oo2pq;
+                    cf[K_W1 + 0] = s.c2a; cf[K_W1 + 1] = s.c2b; cf[K_W1 + 2] = s.c2c; cf[K_W1 + 3] = s.c2d;
+                    c2_boys(c.boys, s.T, L, s.prefac, cf + C2_NCOEF);
                 }
                 __syncthreads();
-                // (ss|ss) top (only when a tag's range starts at s on both sides), in order
-                if(tid == 0)
-                    for(int bb = 0; bb < nb; bb++)
-                        for(int tg = 0; tg < p.ntag; tg++)
-                            if(p.elo[tg] == 0 && p.flo[tg] == 0 && p.ehi[tg] >= 0)
-                                acc[p.acc_off[tg]] += (tg == 0 ? 1.0 : coef[bb * C2_NCOEF + K_W1 + tg - 1]) * wave[bb * W];
-                for(int sf = 1; sf <= p.smax; sf++)
+                for(int b0 = 0; b0 < ng; b0 += B)
                 {
-                    double * cur = wave + (sf % 3) * B * W;
-                    const double * w1 = wave + ((sf + 2) % 3) * B * W;
-                    const double * w2 = wave + ((sf + 1) % 3) * B * W;
-                    for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += nth)
+                    const int nb = min(B, ng - b0);
+                    const double * pb0 = prep + b0 * PS;
+                    // wavefront 0 = block (0,0), m = 0..L
+                    for(int k2 = tid; k2 < nb * (L + 1); k2 += NT)
                     {
-                        const int4 ia = __ldg(p.items + 2 * it);
-                        const int4 ib = __ldg(p.items + 2 * it + 1);
-                        const int x = ib.x & 3;
-                        const bool ket = (ib.x >> 2) & 1;
-                        const int nA = (ib.x >> 3) & 31, nB = (ib.x >> 8) & 255;
-                        const int mlen = ib.x >> 16;
-                        const int gE = ib.y & 0xffff, gF = ib.y >> 16;
+                        const int bb = k2 / (L + 1), n = k2 - bb * (L + 1);
+                        wave[bb * W + n] = pb0[bb * PS + C2_NCOEF + n];
+                    }
+                    // (ss|ss) top (only when a tag's range starts at s on both sides), in order
+                    if(tid == 0)
                         for(int bb = 0; bb < nb; bb++)
+                            for(int tg = 0; tg < (DERIV ? p.ntag : 1); tg++)
+                                if(p.elo[tg] == 0 && p.flo[tg] == 0 && p.ehi[tg] >= 0)
+                                    acc[p.acc_off[tg]] += (tg == 0 ? 1.0 : pb0[bb * PS + K_W1 + tg - 1])
+                                                        * pb0[bb * PS + C2_NCOEF];
+                    __syncthreads();
+                    for(int sf = 1; sf <= p.smax; sf++)
+                    {
+                        double * cur = wave + (sf % 3) * B * W;
+                        const double * w1 = wave + ((sf + 2) % 3) * B * W;
+                        const double * w2 = wave + ((sf + 1) % 3) * B * W;
+                        for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += NT)
                         {
-                            const double * cf = coef + bb * C2_NCOEF;
-                            const double X = cf[(ket ? K_XQ0 : K_XP0) + x];
-                            const double Y = cf[(ket ? K_AOQ0 : K_AOP0) + x];
-                            const double Z = cf[ket ? K_AQ : K_AP];
-                            const double HA = (double)nA * cf[ket ? K_O2Q : K_O2P];
-                            const double HB = (double)nB * cf[K_O2PQ];
-                            const double * s1 = w1 + bb * W + ia.y;
-                            const double * s2 = w2 + bb * W + ia.z;
-                            const double * s3 = w2 + bb * W + ia.w;
-                            double * d = cur + bb * W + ia.x;
-                            for(int m = 0; m < mlen; m++)
+                            const int4 ia = __ldg(&p.items[it].a);
+                            const int4 ib = __ldg(&p.items[it].b);
+                            const double2 nn = __ldg(&p.items[it].c);
+                            const int combo = ib.x & 15;
+                            const int mlen = (ib.x >> 4) & 31;
+                            const bool has2 = (ib.x >> 9) & 1, has3 = (ib.x >> 10) & 1;
+                            const int o2 = has2 ? ia.z : 0, o3 = has3 ? ia.w : 0;
+                            for(int bb = 0; bb < nb; bb++)
                             {
-                                double v = X * s1[m];
-                                v = fma(Y, s1[m + 1], v);
-                                if(ia.z >= 0)
-                                    v = fma(HA, fma(Z, s2[m + 1], s2[m]), v);
-                                if(ia.w >= 0)
-                                    v = fma(HB, s3[m + 1], v);
-                                d[m] = v;
-                            }
-                            // tops: added primitive quartet by primitive quartet, in order
-                            if(ib.z)
-                            {
-                                const double v0 = d[0];
-                                for(int tg = 0; tg < p.ntag; tg++)
-                                    if((ib.z >> tg) & 1)
+                                const double * cf = pb0 + bb * PS;
+                                const double2 XY = *(const double2 *)(cf + 4 * combo);
+                                const double2 ZO = *(const double2 *)(cf + 4 * combo + 2);
+                                const double HA = nn.x * ZO.y;
+                                const double HB = nn.y * cf[K_O2PQ];
+                                const double * s1 = w1 + bb * W + ia.y;
+                                const double * s2 = w2 + bb * W + o2;
+                                const double * s3 = w2 + bb * W + o3;
+                                double * d = cur + bb * W + ia.x;
+                                double a0 = s1[0];
+                                double c0 = has2 ? s2[0] : 0.0;
+                                double v0 = 0.0;
+                                for(int m = 0; m < mlen; m++)
+                                {
+                                    const double a1 = s1[m + 1];
+                                    double v = XY.x * a0;
+                                    v = fma(XY.y, a1, v);
+                                    if(has2)
                                     {
-                                        const int re = gE - c2_lev_off(p.elo[tg]);
-                                        const int rf = gF - c2_lev_off(p.flo[tg]);
-                                        acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf] += (tg == 0 ? v0 : v0 * cf[K_W1 + tg - 1]);
+                                        const double c1 = s2[m + 1];
+                                        v = fma(HA, fma(ZO.x, c1, c0), v);
+                                        c0 = c1;
                                     }
+                                    if(has3)
+                                        v = fma(HB, s3[m + 1], v);
+                                    d[m] = v;
+                                    if(m == 0)
+                                        v0 = v;
+                                    a0 = a1;
+                                }
+                                // tops: added primitive quartet by primitive quartet, in order
+                                if(ib.y >= 0)
+                                    acc[ib.y] += v0;
+                                if(DERIV && ib.z)
+                                {
+                                    const int gE = ib.w & 0xffff, gF = ib.w >> 16;
+                                    for(int tg = 1; tg < p.ntag; tg++)
+                                        if((ib.z >> tg) & 1)
+                                        {
+                                            const int re = gE - c2_lev_off(p.elo[tg]);
+                                            const int rf = gF - c2_lev_off(p.flo[tg]);
+                                            acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf] += v0 * cf[K_W1 + tg - 1];
+                                        }
+                                }
                             }
                         }
+                        __syncthreads();
                     }
-                    __syncthreads();
                 }
             }
-            __syncthreads();      // s_cnt and wcount are reused by the next chunk
+            __syncthreads();      // surv, s_cnt and wcount are reused by the next chunk
         }
         // ---------------- HRR ----------------
-        double * L0 = sm + p.off_hrr;
-        double * L1 = L0 + p.hrr_layer;
+        double * LA = sm + p.off_hrr_b;
+        double * LB = LA + p.hrr_layer;
+        double * mid = sm + p.off_hrr_mid;          // (ab | f) for all columns
         double * o = a.out + off;
-        const int * am = p.am;
-        const int n1 = c2_nc(am[1]), n2 = c2_nc(am[2]), n3 = c2_nc(am[3]);
         for(int ti = 0; ti < p.ntarget; ti++)
         {
             const int * tt = p.tgt[ti];
@@ -349,42 +429,31 @@ __global__ void __launch_bounds__(C2_THREADS) k_coop2(const KernArgs a, const C2
             const int ncol = c2_lev_off(tt[2] + tt[3] + 1) - c2_lev_off(klo);
             const int nbra = c2_nc(tt[0]) * c2_nc(tt[1]);
             const int nket = c2_nc(tt[2]) * c2_nc(tt[3]);
-            double * mid = sm + p.off_hrr + 2 * p.hrr_layer;     // (ab | f) for all columns
             const int accb = p.acc_off[tg], accnf = p.acc_nf[tg];
             const int e0 = c2_lev_off(p.elo[tg]), f0 = c2_lev_off(p.flo[tg]), fk = c2_lev_off(klo);
-            c2_hrr_side(ci, p.brastep_j, tt[0], tt[1], ncol, c.AB[0], c.AB[1], c.AB[2],
-                        [&](int g, int col) { return acc[accb + (g - e0) * accnf + (fk + col - f0)]; },
-                        [&](int r, int col, double v) { mid[r * ncol + col] = v; }, L0, L1);
+            c2_hrr_side<NT>(ci, p.brastep_j, tt[0], tt[1], ncol, c.AB[0], c.AB[1], c.AB[2],
+                            [&](int g, int col) { return acc[accb + (g - e0) * accnf + (fk + col - f0)]; },
+                            [&](int r, int col, double v) { mid[r * ncol + col] = v; }, LA, LB);
             const int kl = c2_lev_off(klo);
             double * resd = res + p.res_off[ti];
-            c2_hrr_side(ci, p.ketstep_l, tt[2], tt[3], nbra, c.CD[0], c.CD[1], c.CD[2],
-                        [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
-                        [&](int r, int row, double v) {
-                            if(p.deriv == 0)
-                            {
-                                // r indexes the ket (c,d) block, row the bra (a,b)
-                                const int pa = row / n1, pb = row % n1, pc = r / n3, pd = r % n3;
-                                const int oi = ((c2_index(ci, c2_lev_off(am[0]) + pa, p.ordering) * n1
-                                                 + c2_index(ci, c2_lev_off(am[1]) + pb, p.ordering)) * n2
-                                                + c2_index(ci, c2_lev_off(am[2]) + pc, p.ordering)) * n3
-                                               + c2_index(ci, c2_lev_off(am[3]) + pd, p.ordering);
-                                o[oi] = v;
-                            }
-                            else
-                                resd[row * nket + r] = v;
-                        }, L0, L1);
+            if(DERIV == 0)
+                c2_hrr_side<NT>(ci, p.ketstep_l, tt[2], tt[3], nbra, c.CD[0], c.CD[1], c.CD[2],
+                                [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
+                                [&](int r, int row, double v) { o[obra[row] + oket[r]] = v; }, LA, LB);
+            else
+                c2_hrr_side<NT>(ci, p.ketstep_l, tt[2], tt[3], nbra, c.CD[0], c.CD[1], c.CD[2],
+                                [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
+                                [&](int r, int row, double v) { resd[row * nket + r] = v; }, LA, LB);
         }
-        if(p.deriv == 1)
+        if(DERIV == 1)
         {
             __syncthreads();
-            const int n0 = c2_nc(am[0]);
-            for(int idx = tid; idx < n0 * n1 * n2 * n3; idx += nth)
+            for(int idx = tid; idx < n0 * n1 * n2 * n3; idx += NT)
             {
                 const int pd = idx % n3, pc = (idx / n3) % n2, pb = (idx / (n3 * n2)) % n1, pa = idx / (n3 * n2 * n1);
                 const int gg[4] = {c2_lev_off(am[0]) + pa, c2_lev_off(am[1]) + pb, c2_lev_off(am[2]) + pc,
                                    c2_lev_off(am[3]) + pd};
-                const int oi = ((c2_index(ci, gg[0], p.ordering) * n1 + c2_index(ci, gg[1], p.ordering)) * n2
-                                + c2_index(ci, gg[2], p.ordering)) * n3 + c2_index(ci, gg[3], p.ordering);
+                const int oi = obra[pa * n1 + pb] + oket[pc * n3 + pd];
                 double g12[12];
                 for(int ctr = 0; ctr < 4; ctr++)
                 {
@@ -453,21 +522,29 @@ static int c2_stepdir(int i, int j, int k)
     return -1;
 }
 
+static bool c2_is_variant(int v) { return v == 21 || v == 22 || v == 24 || v == 41 || v == 42 || v == 44; }
+static int c2_threads(int v) { return v >= 40 ? 128 : 256; }
+
 struct C2Host
 {
     bool ok = false;
+    int nthreads = 256;
     C2Params p;
-    std::vector<int4> items;
-    std::map<int, int4 *> dev_items;     // per device
+    std::vector<C2Item> items;
+    std::map<int, C2Item *> dev_items;     // per device
 };
 
-static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
+// Plan of one class for one variant (v = 0: the default, 256 threads, B = 4
+// halved until shared memory fits).
+static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
 {
     C2Params & p = h.p;
     memset(&p, 0, sizeof(p));
     memcpy(p.am, am, sizeof(p.am));
     p.deriv = deriv;
     p.missing = -1;
+    h.nthreads = v ? c2_threads(v) : 256;
+    const int forceB = v ? v % 20 : 0;
     if(deriv == 0)
     {
         p.ntarget = 1;
@@ -597,7 +674,8 @@ static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
     p.smax = 0;
     for(int s = 1; s <= E + F; s++)
     {
-        p.wstart[s] = (int)h.items.size() / 2;
+        p.wstart[s] = (int)h.items.size();
+        std::vector<C2Item> wv;
         for(int e = std::max(0, s - F); e <= std::min(E, s); e++)
         {
             const int f = s - e;
@@ -613,73 +691,89 @@ static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
                             const int ke = e - ie - je, kf = f - i_f - jf;
                             const int gE = flat(ie, je, ke), gF = flat(i_f, jf, kf);
                             const int E3[3] = {ie, je, ke}, F3[3] = {i_f, jf, kf};
-                            int4 ia, ib;
+                            C2Item itm;
                             int x, nA, nB;
-                            ia.x = slot(e, f, gE, gF);
+                            itm.a.x = slot(e, f, gE, gF);
                             if(ket)
                             {
                                 x = c2_stepdir(i_f, jf, kf);
                                 int f1[3] = {F3[0], F3[1], F3[2]}; f1[x]--;
                                 const int gF1 = flat(f1[0], f1[1], f1[2]);
-                                ia.y = slot(e, f - 1, gE, gF1);
+                                itm.a.y = slot(e, f - 1, gE, gF1);
                                 nA = F3[x] - 1;
                                 if(F3[x] >= 2)
                                 {
                                     int f2[3] = {F3[0], F3[1], F3[2]}; f2[x] -= 2;
-                                    ia.z = slot(e, f - 2, gE, flat(f2[0], f2[1], f2[2]));
+                                    itm.a.z = slot(e, f - 2, gE, flat(f2[0], f2[1], f2[2]));
                                 }
                                 else
-                                    ia.z = -1;
+                                    itm.a.z = -1;
                                 nB = E3[x];
                                 if(E3[x] >= 1)
                                 {
                                     int e1[3] = {E3[0], E3[1], E3[2]}; e1[x]--;
-                                    ia.w = slot(e - 1, f - 1, flat(e1[0], e1[1], e1[2]), gF1);
+                                    itm.a.w = slot(e - 1, f - 1, flat(e1[0], e1[1], e1[2]), gF1);
                                 }
                                 else
-                                    ia.w = -1;
+                                    itm.a.w = -1;
                             }
                             else
                             {
                                 x = c2_stepdir(ie, je, ke);
                                 int e1[3] = {E3[0], E3[1], E3[2]}; e1[x]--;
                                 const int gE1 = flat(e1[0], e1[1], e1[2]);
-                                ia.y = slot(e - 1, f, gE1, gF);
+                                itm.a.y = slot(e - 1, f, gE1, gF);
                                 nA = E3[x] - 1;
                                 if(E3[x] >= 2)
                                 {
                                     int e2[3] = {E3[0], E3[1], E3[2]}; e2[x] -= 2;
-                                    ia.z = slot(e - 2, f, flat(e2[0], e2[1], e2[2]), gF);
+                                    itm.a.z = slot(e - 2, f, flat(e2[0], e2[1], e2[2]), gF);
                                 }
                                 else
-                                    ia.z = -1;
+                                    itm.a.z = -1;
                                 nB = F3[x];
                                 if(F3[x] >= 1)
                                 {
                                     int f1[3] = {F3[0], F3[1], F3[2]}; f1[x]--;
-                                    ia.w = slot(e - 1, f - 1, gE1, flat(f1[0], f1[1], f1[2]));
+                                    itm.a.w = slot(e - 1, f - 1, gE1, flat(f1[0], f1[1], f1[2]));
                                 }
                                 else
-                                    ia.w = -1;
+                                    itm.a.w = -1;
                             }
-                            int mask = 0;
+                            int mask = 0, acc0 = -1;
                             for(int tg = 0; tg < p.ntag; tg++)
                                 if(e >= p.elo[tg] && e <= p.ehi[tg] && f >= p.flo[tg] && f <= p.fhi[tg])
-                                    mask |= 1 << tg;
-                            ib.x = x | ((ket ? 1 : 0) << 2) | (std::max(nA, 0) << 3) | (nB << 8)
-                                 | ((mneed[e][f] + 1) << 16);
-                            ib.y = gE | (gF << 16);
-                            ib.z = mask;
-                            ib.w = 0;
-                            h.items.push_back(ia);
-                            h.items.push_back(ib);
+                                {
+                                    if(tg == 0)
+                                        acc0 = p.acc_off[0] + (gE - lo_h(p.elo[0])) * p.acc_nf[0]
+                                             + (gF - lo_h(p.flo[0]));
+                                    else
+                                        mask |= 1 << tg;
+                                }
+                            const int has2 = itm.a.z >= 0, has3 = itm.a.w >= 0;
+                            itm.b.x = ((ket ? 3 : 0) + x) | ((mneed[e][f] + 1) << 4) | (has2 << 9) | (has3 << 10);
+                            itm.b.y = acc0;
+                            itm.b.z = mask;
+                            itm.b.w = gE | (gF << 16);
+                            itm.c.x = (double)std::max(nA, 0);
+                            itm.c.y = (double)nB;
+                            wv.push_back(itm);
                         }
         }
+        // same shape next to each other: longer m ranges first, then by sources present
+        std::stable_sort(wv.begin(), wv.end(), [](const C2Item & u, const C2Item & w) {
+            const int ku = ((u.b.x >> 4) & 31) * 4 + ((u.b.x >> 9) & 3);
+            const int kw = ((w.b.x >> 4) & 31) * 4 + ((w.b.x >> 9) & 3);
+            return ku > kw;
+        });
+        h.items.insert(h.items.end(), wv.begin(), wv.end());
     }
-    p.wstart[E + F + 1] = (int)h.items.size() / 2;
+    p.wstart[E + F + 1] = (int)h.items.size();
     for(int s = p.smax + 1; s <= E + F + 1; s++)
         p.wstart[s] = p.wstart[E + F + 1];
-    // HRR layer size: the largest layer of either side, over targets
+    // HRR buffers: intermediate layers (not the first, which reads the
+    // accumulators, nor the last, which writes its destination) ping-pong in
+    // two buffers; the bra side's result (ab|f) for all columns sits in mid
     int hl = 0, midmax = 0;
     for(int t = 0; t < p.ntarget; t++)
     {
@@ -689,8 +783,8 @@ static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
         const int nbra = nc2(tt[0]) * nc2(tt[1]);
         auto side = [&](int right, int ta, int tb, int ncl) {
             const int lt = ta + tb, lo = right ? ta : tb, slm = right ? tb : ta;
-            int mx = (lo_h(lt + 1) - lo_h(lo)) * ncl;
-            for(int sl = 1; sl <= slm; sl++)
+            int mx = 0;
+            for(int sl = 1; sl < slm; sl++)
                 mx = std::max(mx, (lo_h(lt - sl + 1) - lo_h(lo)) * nc2(sl) * ncl);
             return mx;
         };
@@ -698,21 +792,25 @@ static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
         hl = std::max(hl, side(p.ketstep_l, tt[2], tt[3], nbra));
         midmax = std::max(midmax, nbra * ncol);
     }
-    p.hrr_layer = hl;
-    // shared memory: [waves | acc | coef | surv] and the HRR [L0 | L1 | mid] reuses waves
+    p.hrr_layer = (hl + 1) & ~1;
+    p.prep_stride = (C2_NCOEF + p.L + 1 + 1) & ~1;
+    // shared memory: [waves | HRR (reuses waves) | acc | prep | surv]
+    const int NT = h.nthreads;
     p.B = forceB > 0 ? forceB : 4;
     for(;;)
     {
         const int waves = 3 * p.B * p.wsize;
-        p.off_acc = std::max(waves, 2 * hl + midmax);
-        p.off_coef = p.off_acc + p.acc_size;
-        p.off_surv = p.off_coef + p.B * C2_NCOEF;
-        p.smem_doubles = p.off_surv + C2_THREADS / 2 + 1;
-        if(p.smem_doubles * 8 <= 200 * 1024 || p.B == 1)
+        const int hrr = 2 * p.hrr_layer + midmax;
+        p.off_hrr_b = 0;
+        p.off_hrr_mid = 2 * p.hrr_layer;
+        p.off_acc = (std::max(waves, hrr) + 1) & ~1;
+        p.off_prep = (p.off_acc + p.acc_size + 1) & ~1;
+        p.off_surv = p.off_prep + C2_SETUP * p.prep_stride;
+        p.smem_doubles = p.off_surv + NT / 2;
+        if(p.smem_doubles * 8 <= 200 * 1024 || p.B == 1 || forceB > 0)
             break;
         p.B /= 2;
     }
-    p.off_hrr = 0;
     p.ordering = 0;
     int ro = 0;
     for(int t = 0; t < p.ntarget; t++)
@@ -722,37 +820,77 @@ static bool c2_build(const int am[4], int deriv, int forceB, C2Host & h)
             ro += nc2(p.tgt[t][0]) * nc2(p.tgt[t][1]) * nc2(p.tgt[t][2]) * nc2(p.tgt[t][3]);
     }
     p.res_size = std::max(ro, 1);
-    return p.smem_doubles * 8 <= 200 * 1024;
+    return p.smem_doubles * 8 <= 200 * 1024 && nc2(am[0]) * nc2(am[1]) <= C2_MAXN
+        && nc2(am[2]) * nc2(am[3]) <= C2_MAXN;
 }
 
 static std::mutex g_c2_mutex;
 static std::map<std::array<int, 6>, C2Host> g_c2;
 
-static C2Host * c2_get(const int am[4], int deriv, int forceB = 0)
+static C2Host * c2_get(const int am[4], int deriv, int v)
 {
     std::lock_guard<std::mutex> lk(g_c2_mutex);
-    std::array<int, 6> key = {am[0], am[1], am[2], am[3], deriv, forceB};
+    std::array<int, 6> key = {am[0], am[1], am[2], am[3], deriv, v};
     auto it = g_c2.find(key);
     if(it == g_c2.end())
     {
         C2Host h;
-        h.ok = c2_build(am, deriv, forceB, h);
-        if(h.ok && forceB > 0 && h.p.B != forceB)
-            h.ok = false;          // that batch size does not fit shared memory
+        h.ok = (v == 0 || c2_is_variant(v)) && c2_build(am, deriv, v, h);
         it = g_c2.emplace(key, std::move(h)).first;
     }
     return &it->second;
 }
 
-bool coop2_supported(const int am[4], int deriv, int forceB)
+bool coop2_supported(const int am[4], int deriv, int v)
 {
-    return c2_get(am, deriv, forceB)->ok;
+    return c2_get(am, deriv, v)->ok;
+}
+
+bool coop2_is_variant(int v) { return c2_is_variant(v); }
+
+template<int MODE, int NT, int DERIV>
+static int c2_launch(KernArgs & a, const C2Params & p, cudaStream_t stream)
+{
+    static std::mutex m;
+    static std::map<std::pair<int, int>, int> per_sm_cache;     // (device, smem) -> CTAs per SM
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = (size_t)p.smem_doubles * sizeof(double);
+    int per_sm = 0, nsm = 148;
+    {
+        std::lock_guard<std::mutex> lk(m);
+        auto it = per_sm_cache.find({dev, (int)smem});
+        if(it == per_sm_cache.end())
+        {
+            cudaFuncSetAttribute(k_coop2<MODE, NT, DERIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop2<MODE, NT, DERIV>, NT, smem) != cudaSuccess)
+            {
+                cudaGetLastError();
+                per_sm = 1;
+            }
+            it = per_sm_cache.emplace(std::make_pair(dev, (int)smem), std::max(per_sm, 1)).first;
+        }
+        per_sm = it->second;
+    }
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long grid = std::min<long long>(a.ntask, (long long)nsm * per_sm);
+    grid = std::max<long long>(grid, 1);
+    Workspace & w = workspace();
+    const size_t scratch = (size_t)grid * p.res_size * sizeof(double);
+    if(!w.dscratch.reserve(scratch))
+    {
+        set_error("out of device memory for cooperative-kernel scratch");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    k_coop2<MODE, NT, DERIV><<<(unsigned)grid, NT, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
+    count_launch(1);
+    return 0;
 }
 
 int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
-                 int forceB)
+                 int v)
 {
-    C2Host * h = c2_get(req, deriv, forceB);
+    C2Host * h = c2_get(req, deriv, v);
     if(!h->ok)
     {
         set_error("class outside the cooperative kernel's range");
@@ -767,14 +905,14 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
         auto it = h->dev_items.find(dev);
         if(it == h->dev_items.end())
         {
-            int4 * d = nullptr;
-            if(cudaMalloc(&d, std::max<size_t>(1, h->items.size()) * sizeof(int4)) != cudaSuccess)
+            C2Item * d = nullptr;
+            if(cudaMalloc(&d, std::max<size_t>(1, h->items.size()) * sizeof(C2Item)) != cudaSuccess)
             {
                 cudaGetLastError();
                 set_error("out of device memory for cooperative-kernel tables");
                 return SIMINT_B200_ERR_CUDA;
             }
-            cudaMemcpy(d, h->items.data(), h->items.size() * sizeof(int4), cudaMemcpyHostToDevice);
+            cudaMemcpy(d, h->items.data(), h->items.size() * sizeof(C2Item), cudaMemcpyHostToDevice);
             it = h->dev_items.emplace(dev, d).first;
         }
         p.items = it->second;
@@ -782,35 +920,20 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
     p.ordering = ordering();
     a.swapB = a.swapK = a.pq = 0;
     a.oidx = nullptr;
-    const size_t smem = (size_t)p.smem_doubles * sizeof(double) + 256;
-    static bool attr[3][2] = {{false, false}, {false, false}, {false, false}};
-    const int mixed = 0;   // the FP32 variant of this kernel is not built yet
-    (void)prec;
-    if(!attr[mode][mixed])
+    (void)prec;      // the VRR of this kernel runs in FP64 for both precision modes
+    if(h->nthreads == 128)
     {
-        if(mode == 0) cudaFuncSetAttribute(k_coop2<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 256);
-        if(mode == 1) cudaFuncSetAttribute(k_coop2<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 256);
-        if(mode == 2) cudaFuncSetAttribute(k_coop2<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024 + 256);
-        attr[mode][mixed] = true;
+        if(deriv)
+            return mode == 0 ? c2_launch<0, 128, 1>(a, p, stream) : mode == 1 ? c2_launch<1, 128, 1>(a, p, stream)
+                                                                 : c2_launch<2, 128, 1>(a, p, stream);
+        return mode == 0 ? c2_launch<0, 128, 0>(a, p, stream) : mode == 1 ? c2_launch<1, 128, 0>(a, p, stream)
+                                                             : c2_launch<2, 128, 0>(a, p, stream);
     }
-    const int per_sm = std::max(1, std::min(4, (int)((220 * 1024) / smem)));
-    long long grid = std::min<long long>(a.ntask, 148LL * per_sm);
-    grid = std::max<long long>(grid, 1);
-    Workspace & w = workspace();
-    const size_t scratch = (size_t)grid * p.res_size * sizeof(double);
-    if(!w.dscratch.reserve(scratch))
-    {
-        set_error("out of device memory for cooperative-kernel scratch");
-        return SIMINT_B200_ERR_CUDA;
-    }
-    if(mode == 0)
-        k_coop2<0, false><<<(unsigned)grid, C2_THREADS, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
-    else if(mode == 1)
-        k_coop2<1, false><<<(unsigned)grid, C2_THREADS, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
-    else
-        k_coop2<2, false><<<(unsigned)grid, C2_THREADS, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
-    count_launch(1);
-    return 0;
+    if(deriv)
+        return mode == 0 ? c2_launch<0, 256, 1>(a, p, stream) : mode == 1 ? c2_launch<1, 256, 1>(a, p, stream)
+                                                             : c2_launch<2, 256, 1>(a, p, stream);
+    return mode == 0 ? c2_launch<0, 256, 0>(a, p, stream) : mode == 1 ? c2_launch<1, 256, 0>(a, p, stream)
+                                                         : c2_launch<2, 256, 0>(a, p, stream);
 }
 
 } // namespace sb200

@@ -491,8 +491,8 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         count_launch(1);
         return 0;
     }
-    if(v >= 20 && coop2_supported(req, deriv, v - 20))
-        return launch_coop2(a, req, deriv, mode, prec, stream, v - 20);
+    if(coop2_is_variant(v) && coop2_supported(req, deriv, v))
+        return launch_coop2(a, req, deriv, mode, prec, stream, v);
     if(v == VAR_COOP1 && coop_supported(req, deriv))
         return launch_coop(a, req, deriv, mode, stream);
     if(v == VAR_GENERIC)
@@ -812,10 +812,9 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case VAR_COOP1:
             ok = coop_supported(am, deriv);
             break;
-        case 21:
-        case 22:
-        case 24:
-            ok = coop2_supported(am, deriv, variant - 20);
+        case 21: case 22: case 24:
+        case 41: case 42: case 44:
+            ok = coop2_supported(am, deriv, variant);
             break;
         default:
             ok = false;

@@ -81,13 +81,16 @@ int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deri
 
 int ncart_of(int l);
 bool coop_supported(const int am[4], int deriv);
-bool coop2_supported(const int am[4], int deriv, int forceB = 0);
+// Cooperative kernel v2; v = 0 for the default plan or a variant code
+// (20 + B: 256 threads, 40 + B: 128 threads; B = 1, 2, 4).
+bool coop2_supported(const int am[4], int deriv, int v = 0);
+bool coop2_is_variant(int v);
 int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
-                 int forceB = 0);
+                 int v = 0);
 
 // Kernel variant per (requested class, deriv, precision), chosen by the
-// autotuner: 0 default rule, 1 straight-line, 2 cooperative v2 (20+B: with
-// batch B), 3 cooperative v1, 4 generic.
+// autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
+// 20+B / 40+B cooperative v2 with batch B and 256 / 128 threads.
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4 };
 int variant_of(const int req[4], int deriv, int prec);
 void set_variant(const int req[4], int deriv, int prec, int v);

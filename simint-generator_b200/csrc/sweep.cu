@@ -575,9 +575,9 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
         std::vector<int> cand;
         if(has_straight(q.req))
             cand.push_back(VAR_STRAIGHT);
-        for(int B : {1, 2, 4})
-            if(coop2_supported(q.req, 0, B))
-                cand.push_back(20 + B);
+        for(int v : {21, 22, 24, 41, 42, 44})
+            if(coop2_supported(q.req, 0, v))
+                cand.push_back(v);
         if(cand.empty())
             continue;
         int best = cand[0];
