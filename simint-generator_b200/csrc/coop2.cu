@@ -8,14 +8,15 @@
 // centre order OSTEI_VRR_Algorithm_Base.cpp:449-469).  Blocks are grouped
 // into anti-diagonal wavefronts s = e+f (a block depends only on s-1 and
 // s-2) and each block keeps only the auxiliary orders m it really feeds.
-// Inside a wavefront the items are sorted by shape (m count, which sources
-// exist) so the threads of a warp take the same branches.
+// An item is one auxiliary order m of one element, so the (independent)
+// orders of an element spread over threads; items keep the natural order so
+// neighbouring threads touch neighbouring shared-memory words.
 //
 // Surviving primitive quartets (the reference's screening tests) are
 // compacted in order; their set-up and Boys values are computed 16 at a time
 // by 16 threads into shared memory, then processed B at a time: a thread
-// owns an item and runs it for all B primitive quartets and all its m
-// values, so one __syncthreads per wavefront serves B primitive quartets.
+// owns an item and runs it for all B primitive quartets, so one
+// __syncthreads per wavefront serves B primitive quartets.
 // Per primitive quartet the step coefficients are stored as six
 // (direction, side) combos of [X, Y, Z, 1/2s] so an item reads its four
 // coefficients with two 16-byte loads.  Top quartets are summed into
@@ -51,13 +52,15 @@
 
 enum { K_O2PQ = 24, K_W1 = 25 };
 
-struct C2Item
-{
-    int4 a;                  // dst, src1, src2, src3 (offsets of the m = 0 slot; -1 = none)
-    int4 b;                  // combo | mlen << 4 | has2 << 9 | has3 << 10,  acc index of tag 0 (-1 = none),
-                             // mask of tags >= 1,  gE | gF << 16
-    double2 c;               // nA, nB (integer factors of the 1/2p and 1/2(p+q) terms)
-};
+// One VRR item, 16 bytes:
+//   x = dst | src1 << 16                  (offsets of the m = 0 slots in a wave buffer)
+//   y = src2 | src3 << 16                 (0 when absent)
+//   z = acc index of tag 0 (0xffff = none) | combo << 16 | has2 << 24 | has3 << 25
+//       | (mask of tags 1..4) << 26
+// One unit computes one auxiliary order m of one element (m is folded into
+// the offsets).
+//   w = nA | nB << 4 | gE << 8 | gF << 18 (integer factors; Cartesian indices of deriv tags)
+typedef int4 C2Item;
 
 struct C2Params
 {
@@ -355,53 +358,41 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
                         const double * w2 = wave + ((sf + 1) % 3) * B * W;
                         for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += NT)
                         {
-                            const int4 ia = __ldg(&p.items[it].a);
-                            const int4 ib = __ldg(&p.items[it].b);
-                            const double2 nn = __ldg(&p.items[it].c);
-                            const int combo = ib.x & 15;
-                            const int mlen = (ib.x >> 4) & 31;
-                            const bool has2 = (ib.x >> 9) & 1, has3 = (ib.x >> 10) & 1;
-                            const int o2 = has2 ? ia.z : 0, o3 = has3 ? ia.w : 0;
+                            const int4 q = __ldg(&p.items[it]);
+                            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
+                            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
+                            const int acc0 = q.z & 0xffff;
+                            const int combo = (q.z >> 16) & 7;
+                            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
+                            const int tmask = ((q.z >> 26) & 15) << 1;
+                            const double dA = (double)(q.w & 15), dB = (double)((q.w >> 4) & 15);
                             for(int bb = 0; bb < nb; bb++)
                             {
                                 const double * cf = pb0 + bb * PS;
                                 const double2 XY = *(const double2 *)(cf + 4 * combo);
                                 const double2 ZO = *(const double2 *)(cf + 4 * combo + 2);
-                                const double HA = nn.x * ZO.y;
-                                const double HB = nn.y * cf[K_O2PQ];
-                                const double * s1 = w1 + bb * W + ia.y;
+                                const double HA = dA * ZO.y;
+                                const double HB = dB * cf[K_O2PQ];
+                                const double * s1 = w1 + bb * W + o1;
                                 const double * s2 = w2 + bb * W + o2;
                                 const double * s3 = w2 + bb * W + o3;
-                                double * d = cur + bb * W + ia.x;
-                                double a0 = s1[0];
-                                double c0 = has2 ? s2[0] : 0.0;
-                                double v0 = 0.0;
-                                for(int m = 0; m < mlen; m++)
-                                {
-                                    const double a1 = s1[m + 1];
-                                    double v = XY.x * a0;
-                                    v = fma(XY.y, a1, v);
-                                    if(has2)
-                                    {
-                                        const double c1 = s2[m + 1];
-                                        v = fma(HA, fma(ZO.x, c1, c0), v);
-                                        c0 = c1;
-                                    }
-                                    if(has3)
-                                        v = fma(HB, s3[m + 1], v);
-                                    d[m] = v;
-                                    if(m == 0)
-                                        v0 = v;
-                                    a0 = a1;
-                                }
+                                double * d = cur + bb * W + dsto;
+                                double v = XY.x * s1[0];
+                                v = fma(XY.y, s1[1], v);
+                                if(has2)
+                                    v = fma(HA, fma(ZO.x, s2[1], s2[0]), v);
+                                if(has3)
+                                    v = fma(HB, s3[1], v);
+                                d[0] = v;
+                                const double v0 = v;
                                 // tops: added primitive quartet by primitive quartet, in order
-                                if(ib.y >= 0)
-                                    acc[ib.y] += v0;
-                                if(DERIV && ib.z)
+                                if(acc0 != 0xffff)
+                                    acc[acc0] += v0;
+                                if(DERIV && tmask)
                                 {
-                                    const int gE = ib.w & 0xffff, gF = ib.w >> 16;
+                                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
                                     for(int tg = 1; tg < p.ntag; tg++)
-                                        if((ib.z >> tg) & 1)
+                                        if((tmask >> tg) & 1)
                                         {
                                             const int re = gE - c2_lev_off(p.elo[tg]);
                                             const int rf = gF - c2_lev_off(p.flo[tg]);
@@ -524,6 +515,11 @@ static int c2_stepdir(int i, int j, int k)
 
 static bool c2_is_variant(int v) { return v == 21 || v == 22 || v == 24 || v == 41 || v == 42 || v == 44; }
 static int c2_threads(int v) { return v >= 40 ? 128 : 256; }
+
+struct C2ItemHost
+{
+    int dst, s1, s2, s3, combo, mlen, acc0, mask, gE, gF, nA, nB;
+};
 
 struct C2Host
 {
@@ -675,7 +671,7 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
     for(int s = 1; s <= E + F; s++)
     {
         p.wstart[s] = (int)h.items.size();
-        std::vector<C2Item> wv;
+        std::vector<C2ItemHost> wv;
         for(int e = std::max(0, s - F); e <= std::min(E, s); e++)
         {
             const int f = s - e;
@@ -691,54 +687,54 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
                             const int ke = e - ie - je, kf = f - i_f - jf;
                             const int gE = flat(ie, je, ke), gF = flat(i_f, jf, kf);
                             const int E3[3] = {ie, je, ke}, F3[3] = {i_f, jf, kf};
-                            C2Item itm;
+                            C2ItemHost itm;
                             int x, nA, nB;
-                            itm.a.x = slot(e, f, gE, gF);
+                            itm.dst = slot(e, f, gE, gF);
                             if(ket)
                             {
                                 x = c2_stepdir(i_f, jf, kf);
                                 int f1[3] = {F3[0], F3[1], F3[2]}; f1[x]--;
                                 const int gF1 = flat(f1[0], f1[1], f1[2]);
-                                itm.a.y = slot(e, f - 1, gE, gF1);
+                                itm.s1 = slot(e, f - 1, gE, gF1);
                                 nA = F3[x] - 1;
                                 if(F3[x] >= 2)
                                 {
                                     int f2[3] = {F3[0], F3[1], F3[2]}; f2[x] -= 2;
-                                    itm.a.z = slot(e, f - 2, gE, flat(f2[0], f2[1], f2[2]));
+                                    itm.s2 = slot(e, f - 2, gE, flat(f2[0], f2[1], f2[2]));
                                 }
                                 else
-                                    itm.a.z = -1;
+                                    itm.s2 = -1;
                                 nB = E3[x];
                                 if(E3[x] >= 1)
                                 {
                                     int e1[3] = {E3[0], E3[1], E3[2]}; e1[x]--;
-                                    itm.a.w = slot(e - 1, f - 1, flat(e1[0], e1[1], e1[2]), gF1);
+                                    itm.s3 = slot(e - 1, f - 1, flat(e1[0], e1[1], e1[2]), gF1);
                                 }
                                 else
-                                    itm.a.w = -1;
+                                    itm.s3 = -1;
                             }
                             else
                             {
                                 x = c2_stepdir(ie, je, ke);
                                 int e1[3] = {E3[0], E3[1], E3[2]}; e1[x]--;
                                 const int gE1 = flat(e1[0], e1[1], e1[2]);
-                                itm.a.y = slot(e - 1, f, gE1, gF);
+                                itm.s1 = slot(e - 1, f, gE1, gF);
                                 nA = E3[x] - 1;
                                 if(E3[x] >= 2)
                                 {
                                     int e2[3] = {E3[0], E3[1], E3[2]}; e2[x] -= 2;
-                                    itm.a.z = slot(e - 2, f, flat(e2[0], e2[1], e2[2]), gF);
+                                    itm.s2 = slot(e - 2, f, flat(e2[0], e2[1], e2[2]), gF);
                                 }
                                 else
-                                    itm.a.z = -1;
+                                    itm.s2 = -1;
                                 nB = F3[x];
                                 if(F3[x] >= 1)
                                 {
                                     int f1[3] = {F3[0], F3[1], F3[2]}; f1[x]--;
-                                    itm.a.w = slot(e - 1, f - 1, gE1, flat(f1[0], f1[1], f1[2]));
+                                    itm.s3 = slot(e - 1, f - 1, gE1, flat(f1[0], f1[1], f1[2]));
                                 }
                                 else
-                                    itm.a.w = -1;
+                                    itm.s3 = -1;
                             }
                             int mask = 0, acc0 = -1;
                             for(int tg = 0; tg < p.ntag; tg++)
@@ -750,23 +746,49 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
                                     else
                                         mask |= 1 << tg;
                                 }
-                            const int has2 = itm.a.z >= 0, has3 = itm.a.w >= 0;
-                            itm.b.x = ((ket ? 3 : 0) + x) | ((mneed[e][f] + 1) << 4) | (has2 << 9) | (has3 << 10);
-                            itm.b.y = acc0;
-                            itm.b.z = mask;
-                            itm.b.w = gE | (gF << 16);
-                            itm.c.x = (double)std::max(nA, 0);
-                            itm.c.y = (double)nB;
-                            wv.push_back(itm);
+                            itm.combo = (ket ? 3 : 0) + x;
+                            itm.mlen = mneed[e][f] + 1;
+                            itm.acc0 = acc0;
+                            itm.mask = mask;
+                            itm.gE = gE;
+                            itm.gF = gF;
+                            itm.nA = std::max(nA, 0);
+                            itm.nB = nB;
+                            // one unit per auxiliary order m: the orders of an element are
+                            // independent, so they spread over threads instead of
+                            // running as one serial chain
+                            for(int m = 0; m < itm.mlen; m++)
+                            {
+                                C2ItemHost u = itm;
+                                u.dst += m;
+                                u.s1 += m;
+                                if(u.s2 >= 0) u.s2 += m;
+                                if(u.s3 >= 0) u.s3 += m;
+                                u.mlen = 1;
+                                if(m > 0)
+                                {
+                                    u.acc0 = -1;
+                                    u.mask = 0;
+                                }
+                                wv.push_back(u);
+                            }
                         }
         }
-        // same shape next to each other: longer m ranges first, then by sources present
-        std::stable_sort(wv.begin(), wv.end(), [](const C2Item & u, const C2Item & w) {
-            const int ku = ((u.b.x >> 4) & 31) * 4 + ((u.b.x >> 9) & 3);
-            const int kw = ((w.b.x >> 4) & 31) * 4 + ((w.b.x >> 9) & 3);
-            return ku > kw;
-        });
-        h.items.insert(h.items.end(), wv.begin(), wv.end());
+        // natural order (block by block, element by element, m innermost):
+        // neighbouring threads touch neighbouring shared-memory words
+        for(const C2ItemHost & u : wv)
+        {
+            if(u.dst >= 65536 || u.s1 >= 65536 || u.s2 >= 65536 || u.s3 >= 65536 || u.acc0 >= 65535
+               || u.nA > 15 || u.nB > 15 || u.gE >= 1024 || u.gF >= 1024 || u.mlen != 1)
+                return false;            // outside the packed item format
+            C2Item q;
+            q.x = (int)((unsigned)u.dst | ((unsigned)u.s1 << 16));
+            q.y = (int)((unsigned)(u.s2 < 0 ? 0 : u.s2) | ((unsigned)(u.s3 < 0 ? 0 : u.s3) << 16));
+            q.z = (u.acc0 < 0 ? 0xffff : u.acc0) | (u.combo << 16) | ((u.s2 >= 0) << 24)
+                | ((u.s3 >= 0) << 25) | (((u.mask >> 1) & 15) << 26);
+            q.w = u.nA | (u.nB << 4) | (u.gE << 8) | (u.gF << 18);
+            h.items.push_back(q);
+        }
     }
     p.wstart[E + F + 1] = (int)h.items.size();
     for(int s = p.smax + 1; s <= E + F + 1; s++)

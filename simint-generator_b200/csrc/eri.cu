@@ -476,7 +476,7 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         // untuned default: the register kernel while its contracted tops fit
         // registers (above ~200 accumulators it spills), else cooperative
         v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
-    if(v == VAR_STRAIGHT && k)
+    if((v == VAR_STRAIGHT || v == VAR_STRAIGHT64) && k)
     {
         a.oidx = oidx_table(req, u, ordering());
         if(!a.oidx)
@@ -486,7 +486,7 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         }
         const int threads = 128;
         const long long blocks = (a.ntask + threads - 1) / threads;
-        KernFn fn = k->fn[mode][prec == SIMINT_B200_PREC_MIXED ? 1 : 0];
+        KernFn fn = k->fn[mode][(prec == SIMINT_B200_PREC_MIXED && v == VAR_STRAIGHT) ? 1 : 0];
         fn<<<(unsigned)blocks, threads, 0, stream>>>(a);
         count_launch(1);
         return 0;
@@ -807,6 +807,7 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
             ok = true;
             break;
         case VAR_STRAIGHT:
+        case VAR_STRAIGHT64:
             ok = deriv == 0 && has_straight(am);
             break;
         case VAR_COOP1:

@@ -574,7 +574,11 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
             continue;
         std::vector<int> cand;
         if(has_straight(q.req))
+        {
             cand.push_back(VAR_STRAIGHT);
+            if(prec == SIMINT_B200_PREC_MIXED)
+                cand.push_back(VAR_STRAIGHT64);
+        }
         for(int v : {21, 22, 24, 41, 42, 44})
             if(coop2_supported(q.req, 0, v))
                 cand.push_back(v);
