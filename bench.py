@@ -9,8 +9,10 @@ sweep (1.9e9 quartets, 1e11 primitive quartets) is far beyond one step, so a
 step is one pass over a proportional stratified subsample of it: every
 `--stride`-th bra-pair row of every AM class (the class mix of the whole
 sweep is kept).  Metric: evaluated primitive quartets per second.  `value`
-is the mixed-precision batched path (FP32 VRR where the Schwarz bound allows,
-FP64 elsewhere); the FP64 path is reported beside it.
+is the mixed-precision batched path (FP32 VRR for primitive quartets whose
+estimated FP32 error is below the gate, FP64 elsewhere); the FP64 path is
+reported beside it, with the mixed path's max absolute and relative
+deviation from it per class.
 
 Arms:
   default            B200 sweep (device-resident inputs; CUDA-graph replay),
@@ -55,8 +57,9 @@ def parse():
     ap.add_argument("--stride", type=int, default=2000,
                     help="keep every stride-th bra-pair row of each class")
     ap.add_argument("--e2e-stride", type=int, default=40000)
-    ap.add_argument("--gate", type=float, default=None,
-                    help="mixed-precision Schwarz-bound gate (default: from the error model)")
+    ap.add_argument("--gate", type=float, default=1e-8,
+                    help="mixed precision: FP32 VRR for primitive quartets whose estimated FP32 "
+                         "error is below this (simint_b200_set_precision)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -250,7 +253,7 @@ def run_b200(args):
     flush = torch.empty((256 << 20) // 4, dtype=torch.float32, device="cuda")   # > L2 (126 MB)
     peak64 = sb.fma_peak(False, lib)
     peak32 = sb.fma_peak(True, lib)
-    gate = args.gate if args.gate is not None else 1e-6
+    gate = args.gate
     # autotune kernel variants per class on this sweep (untimed)
     t1 = time.time()
     for prec in (sb.FP64, sb.MIXED):
@@ -297,9 +300,25 @@ def run_b200(args):
     sumsmx = B.checksums()
     lib.simint_b200_set_precision(sb.FP64, 0.0)
     ct64 = B.class_times(sb.FP64, out.data_ptr(), cap, stream.cuda_stream)
+    full = B.output_size <= cap
+    out64 = out.clone() if full else None
     lib.simint_b200_set_precision(sb.MIXED, gate)
     ctmx = B.class_times(sb.MIXED, out.data_ptr(), cap, stream.cuda_stream)
     lib.simint_b200_set_precision(sb.FP64, 0.0)
+    torch.cuda.synchronize()
+    # deviation of the mixed path from the FP64 path, per class (full-layout
+    # output only); relative error over elements above 1e-10 of the class max
+    errs = {}
+    if full:
+        for k, c in enumerate(classes):
+            a, n = c["offset"], c["nquart"] * c["nout"]
+            if n == 0:
+                continue
+            d = (out[a:a + n] - out64[a:a + n]).abs()
+            ref = out64[a:a + n].abs()
+            big = ref > 1e-10 * float(ref.max())
+            errs[k] = (float(d.max()), float((d[big] / ref[big]).max()) if bool(big.any()) else 0.0)
+        del out64
     total_npq = npq
     if dist:
         tt = torch.tensor([float(npq)], device="cuda", dtype=torch.float64)
@@ -318,7 +337,9 @@ def run_b200(args):
                           "fp64_tflops": fl / max(ct64[k], 1e-9) / 1e9,
                           "checksum_fp64": float(sums64[k, 0]), "checksum_mixed": float(sumsmx[k, 0]),
                           "abssum_fp64": float(sums64[k, 1]),
-                          "variant_fp64": B.variant(c["am"], sb.FP64), "variant_mixed": B.variant(c["am"], sb.MIXED)})
+                          "variant_fp64": B.variant(c["am"], sb.FP64), "variant_mixed": B.variant(c["am"], sb.MIXED),
+                          "mixed_max_abs_err": errs.get(k, (None, None))[0],
+                          "mixed_max_rel_err": errs.get(k, (None, None))[1]})
     dom = max(range(len(classes)), key=lambda k: ctmx[k])
     dc = classes[dom]
     dom_fl = flops_of_class(dc["am"], dc["nprimq"], dc["nquart"])
@@ -371,7 +392,7 @@ def run_b200(args):
             "metric": "primitive quartets/s, mixed-precision batched sweep (cfg2 l<=3, screen 1e-14)",
             "value": value, "unit": "primitive quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the Schwarz gate)",
+            "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the error-estimate gate)",
             "data": "synthetic (seeded cfg2 shells, PCG64 seed 2024)",
             "config": {"workload": "cfg2 sweep sample: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, "
                                    "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14; every %d-th bra "
@@ -381,6 +402,9 @@ def run_b200(args):
                        "gate": gate, "l2": "256 MB flush before every timed step",
                        "parallelism": "dp%d (disjoint row shards)" % world, "setup_s": round(setup_s, 1), "autotune_s": round(tune_s, 1)},
             "fp64": {"value": value64, "ms_per_step": ms64},
+            "mixed_vs_fp64": {"max_abs_err": max((e[0] for e in errs.values()), default=None),
+                              "max_rel_err": max((e[1] for e in errs.values()), default=None),
+                              "bar_abs": 1e-10, "classes_checked": len(errs)},
             "roofline": {"bound": "fp64", "kernel": "class " + "".join("spdfg"[x] for x in dc["am"]),
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 > 0 else None, "traffic": traffic,

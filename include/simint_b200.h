@@ -35,10 +35,17 @@ extern "C" {
 int simint_b200_set_ordering(int ordering);
 int simint_b200_get_ordering(void);
 
-/* FP64 everywhere, or FP32 VRR for primitive quartets whose Schwarz bound
- * sqrt(screen_ab * screen_cd) is below `gate` (FP64 Boys, prefactors,
- * contraction and HRR in both modes).  Applies to pairs built with Schwarz
- * screening; others always run in FP64.  Process-wide. */
+/* FP64 everywhere, or FP32 VRR for primitive quartets whose estimated FP32
+ * error is below `gate` (FP64 Boys, prefactors, contraction and HRR in both
+ * modes).  The estimate of one primitive quartet of a class with recursion
+ * depth L = la+lb+lc+ld is
+ *     8 (L+1) 2^-24 |prefac| r^L (1 + |AB|)^min(la,lb) (1 + |CD|)^min(lc,ld),
+ *     r = (g + sqrt(g^2 + 4h)) / 2,  g = 1 + max|X| + max|Y|,
+ *     h = L (1/2p + 1/2q + 1/2(p+q))
+ * (X: P-A, P-B, Q-C, Q-D components; Y: the rho/p, rho/q (P-Q) terms), a
+ * bound on the absolute error its FP32 VRR adds to any integral of the
+ * shell quartet; an integral's error is at most the sum over its primitive
+ * quartets.  gate = 0 keeps FP64.  Process-wide. */
 int simint_b200_set_precision(int mode, double gate);
 int simint_b200_get_precision(void);
 

@@ -77,6 +77,7 @@ struct C2Params
     const C2Item * items;
     int off_acc, off_prep, off_surv, off_hrr_b, off_hrr_mid;   // shared-memory layout (doubles)
     int prep_stride;              // doubles per prepared primitive quartet
+    int off32;                    // offset (doubles) of its FP32 coefficient copy
     int hrr_layer;                // doubles per HRR layer buffer
     int smem_doubles;
     int ordering;
@@ -229,7 +230,101 @@ __device__ __forceinline__ void c2_boys(const double * __restrict__ tab, double 
     }
 }
 
-template<int MODE, int NT, int DERIV>
+// Coefficient combo of one prepared primitive quartet: X, Y, Z, 1/2s.
+__device__ __forceinline__ void c2_combo(const double * cf, int combo, double & X, double & Y, double & Z, double & O)
+{
+    const double2 XY = *(const double2 *)(cf + 4 * combo);
+    const double2 ZO = *(const double2 *)(cf + 4 * combo + 2);
+    X = XY.x; Y = XY.y; Z = ZO.x; O = ZO.y;
+}
+
+__device__ __forceinline__ void c2_combo(const float * cf, int combo, float & X, float & Y, float & Z, float & O)
+{
+    const float4 q = *(const float4 *)(cf + 4 * combo);
+    X = q.x; Y = q.y; Z = q.z; O = q.w;
+}
+
+// The VRR of nb primitive quartets (prepared slots slot[0..nb)) in type T,
+// wavefront by wavefront, with the tops added to the FP64 accumulators in
+// slot order.  wave holds 3 wavefronts x cap batch entries x W values of T.
+template<typename T, int NT, int DERIV>
+__device__ __forceinline__ void c2_batch(const C2Params & p, T * __restrict__ wave, int cap, int W,
+                                         const double * __restrict__ prep, int PS, int off32,
+                                         const int * __restrict__ slot, int nb, double * __restrict__ acc)
+{
+    const int tid = threadIdx.x;
+    const int L = p.L;
+    // wavefront 0 = block (0,0), m = 0..L
+    for(int k2 = tid; k2 < nb * (L + 1); k2 += NT)
+    {
+        const int bb = k2 / (L + 1), n = k2 - bb * (L + 1);
+        wave[bb * W + n] = (T)prep[slot[bb] * PS + C2_NCOEF + n];
+    }
+    // (ss|ss) top (only when a tag's range starts at s on both sides), in order
+    if(tid == 0)
+        for(int bb = 0; bb < nb; bb++)
+        {
+            const double * cf = prep + slot[bb] * PS;
+            for(int tg = 0; tg < (DERIV ? p.ntag : 1); tg++)
+                if(p.elo[tg] == 0 && p.flo[tg] == 0 && p.ehi[tg] >= 0)
+                    acc[p.acc_off[tg]] += (tg == 0 ? 1.0 : cf[K_W1 + tg - 1]) * cf[C2_NCOEF];
+        }
+    __syncthreads();
+    for(int sf = 1; sf <= p.smax; sf++)
+    {
+        T * cur = wave + (sf % 3) * cap * W;
+        const T * w1 = wave + ((sf + 2) % 3) * cap * W;
+        const T * w2 = wave + ((sf + 1) % 3) * cap * W;
+        for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += NT)
+        {
+            const int4 q = __ldg(&p.items[it]);
+            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
+            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
+            const int acc0 = q.z & 0xffff;
+            const int combo = (q.z >> 16) & 7;
+            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
+            const int tmask = ((q.z >> 26) & 15) << 1;
+            const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
+            for(int bb = 0; bb < nb; bb++)
+            {
+                const double * cfd = prep + slot[bb] * PS;
+                const T * cf = (const T *)(cfd + off32);
+                T X, Y, Z, O;
+                c2_combo(cf, combo, X, Y, Z, O);
+                const T HA = dA * O;
+                const T HB = dB * cf[K_O2PQ];
+                const T * s1 = w1 + bb * W + o1;
+                const T * s2 = w2 + bb * W + o2;
+                const T * s3 = w2 + bb * W + o3;
+                T v = X * s1[0];
+                v = fma(Y, s1[1], v);
+                if(has2)
+                    v = fma(HA, fma(Z, s2[1], s2[0]), v);
+                if(has3)
+                    v = fma(HB, s3[1], v);
+                cur[bb * W + dsto] = v;
+                // tops: added primitive quartet by primitive quartet, in order
+                const double v0 = (double)v;
+                if(acc0 != 0xffff)
+                    acc[acc0] += v0;
+                if(DERIV && tmask)
+                {
+                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
+                    for(int tg = 1; tg < p.ntag; tg++)
+                        if((tmask >> tg) & 1)
+                        {
+                            const int re = gE - c2_lev_off(p.elo[tg]);
+                            const int rf = gF - c2_lev_off(p.flo[tg]);
+                            acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf] += v0 * cfd[K_W1 + tg - 1];
+                        }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template<int MODE, int NT, int DERIV, bool MIXED>
 __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs a, const C2Params p,
                                                                  double * __restrict__ gres)
 {
@@ -238,6 +333,8 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
     __shared__ int s_cnt;
     __shared__ int wcount[NT / 32];
     __shared__ int obra[C2_MAXN], oket[C2_MAXN];
+    __shared__ int s_slot[C2_SETUP];
+    __shared__ int s_nhigh;
     const int tid = threadIdx.x;
     for(int k = tid; k < CI_NCART; k += NT)
         ci[k] = c_cartinfo[k];
@@ -266,6 +363,11 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
         task_of<MODE>(a, t, iP, iQ, off);
         QuartetCtx c;
         make_ctx(a, iP, iQ, c);
+        if(MIXED)
+        {
+            c.gL = L;
+            c.gamp = hrr_amp(c, min(am[0], am[1]), min(am[2], am[3]));
+        }
         for(int k = tid; k < p.acc_size; k += NT)
             acc[k] = 0.0;
         const int ni = c.bi1 - c.bi0, nj = c.kj1 - c.kj0;
@@ -306,6 +408,7 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
             {
                 const int ng = min(C2_SETUP, nsurv - g0);
                 // set-up and Boys of up to C2_SETUP primitive quartets in parallel
+                bool low = false;
                 if(tid < ng)
                 {
                     const int kk = surv[g0 + tid];
@@ -331,79 +434,40 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
                     cf[K_O2PQ] = s.oo2pq;
                     cf[K_W1 + 0] = s.c2a; cf[K_W1 + 1] = s.c2b; cf[K_W1 + 2] = s.c2c; cf[K_W1 + 3] = s.c2d;
                     c2_boys(c.boys, s.T, L, s.prefac, cf + C2_NCOEF);
+                    if(MIXED)
+                    {
+                        low = s.lowprec;
+                        float * f32 = (float *)(cf + p.off32);
+                        #pragma unroll
+                        for(int k2 = 0; k2 <= K_O2PQ; k2++)
+                            f32[k2] = (float)cf[k2];
+                    }
                 }
-                __syncthreads();
-                for(int b0 = 0; b0 < ng; b0 += B)
+                if(MIXED)
                 {
-                    const int nb = min(B, ng - b0);
-                    const double * pb0 = prep + b0 * PS;
-                    // wavefront 0 = block (0,0), m = 0..L
-                    for(int k2 = tid; k2 < nb * (L + 1); k2 += NT)
+                    // FP64 primitive quartets first, then the FP32 ones, each in order
+                    if(tid < 32)
                     {
-                        const int bb = k2 / (L + 1), n = k2 - bb * (L + 1);
-                        wave[bb * W + n] = pb0[bb * PS + C2_NCOEF + n];
-                    }
-                    // (ss|ss) top (only when a tag's range starts at s on both sides), in order
-                    if(tid == 0)
-                        for(int bb = 0; bb < nb; bb++)
-                            for(int tg = 0; tg < (DERIV ? p.ntag : 1); tg++)
-                                if(p.elo[tg] == 0 && p.flo[tg] == 0 && p.ehi[tg] >= 0)
-                                    acc[p.acc_off[tg]] += (tg == 0 ? 1.0 : pb0[bb * PS + K_W1 + tg - 1])
-                                                        * pb0[bb * PS + C2_NCOEF];
-                    __syncthreads();
-                    for(int sf = 1; sf <= p.smax; sf++)
-                    {
-                        double * cur = wave + (sf % 3) * B * W;
-                        const double * w1 = wave + ((sf + 2) % 3) * B * W;
-                        const double * w2 = wave + ((sf + 1) % 3) * B * W;
-                        for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += NT)
-                        {
-                            const int4 q = __ldg(&p.items[it]);
-                            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
-                            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
-                            const int acc0 = q.z & 0xffff;
-                            const int combo = (q.z >> 16) & 7;
-                            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
-                            const int tmask = ((q.z >> 26) & 15) << 1;
-                            const double dA = (double)(q.w & 15), dB = (double)((q.w >> 4) & 15);
-                            for(int bb = 0; bb < nb; bb++)
-                            {
-                                const double * cf = pb0 + bb * PS;
-                                const double2 XY = *(const double2 *)(cf + 4 * combo);
-                                const double2 ZO = *(const double2 *)(cf + 4 * combo + 2);
-                                const double HA = dA * ZO.y;
-                                const double HB = dB * cf[K_O2PQ];
-                                const double * s1 = w1 + bb * W + o1;
-                                const double * s2 = w2 + bb * W + o2;
-                                const double * s3 = w2 + bb * W + o3;
-                                double * d = cur + bb * W + dsto;
-                                double v = XY.x * s1[0];
-                                v = fma(XY.y, s1[1], v);
-                                if(has2)
-                                    v = fma(HA, fma(ZO.x, s2[1], s2[0]), v);
-                                if(has3)
-                                    v = fma(HB, s3[1], v);
-                                d[0] = v;
-                                const double v0 = v;
-                                // tops: added primitive quartet by primitive quartet, in order
-                                if(acc0 != 0xffff)
-                                    acc[acc0] += v0;
-                                if(DERIV && tmask)
-                                {
-                                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
-                                    for(int tg = 1; tg < p.ntag; tg++)
-                                        if((tmask >> tg) & 1)
-                                        {
-                                            const int re = gE - c2_lev_off(p.elo[tg]);
-                                            const int rf = gF - c2_lev_off(p.flo[tg]);
-                                            acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf] += v0 * cf[K_W1 + tg - 1];
-                                        }
-                                }
-                            }
-                        }
-                        __syncthreads();
+                        const unsigned lowm = __ballot_sync(0xffffffffu, low);
+                        const unsigned valid = ng >= 32 ? 0xffffffffu : ((1u << ng) - 1u);
+                        const unsigned lt = (1u << (tid & 31)) - 1u;
+                        const int nhigh = __popc(valid & ~lowm);
+                        if(tid < ng)
+                            s_slot[low ? nhigh + __popc(lowm & valid & lt) : __popc(valid & ~lowm & lt)] = tid;
+                        if(tid == 0)
+                            s_nhigh = nhigh;
                     }
                 }
+                else if(tid < ng)
+                    s_slot[tid] = tid;
+                __syncthreads();
+                const int nhigh = MIXED ? s_nhigh : ng;
+                for(int b0 = 0; b0 < nhigh; b0 += B)
+                    c2_batch<double, NT, DERIV>(p, wave, B, W, prep, PS, 0, s_slot + b0, min(B, nhigh - b0), acc);
+                if(MIXED)
+                    for(int b0 = nhigh; b0 < ng; b0 += 2 * B)
+                        c2_batch<float, NT, DERIV>(p, (float *)wave, 2 * B, W, prep, PS, p.off32, s_slot + b0,
+                                                   min(2 * B, ng - b0), acc);
             }
             __syncthreads();      // surv, s_cnt and wcount are reused by the next chunk
         }
@@ -815,7 +879,10 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
         midmax = std::max(midmax, nbra * ncol);
     }
     p.hrr_layer = (hl + 1) & ~1;
-    p.prep_stride = (C2_NCOEF + p.L + 1 + 1) & ~1;
+    // prepared primitive quartet: FP64 coefficients and Boys values, then an
+    // FP32 copy of the coefficients (25 floats) for the mixed-precision VRR
+    p.off32 = (C2_NCOEF + p.L + 1 + 1) & ~1;
+    p.prep_stride = p.off32 + 14;
     // shared memory: [waves | HRR (reuses waves) | acc | prep | surv]
     const int NT = h.nthreads;
     p.B = forceB > 0 ? forceB : 4;
@@ -870,7 +937,7 @@ bool coop2_supported(const int am[4], int deriv, int v)
 
 bool coop2_is_variant(int v) { return c2_is_variant(v); }
 
-template<int MODE, int NT, int DERIV>
+template<int MODE, int NT, int DERIV, bool MIXED>
 static int c2_launch(KernArgs & a, const C2Params & p, cudaStream_t stream)
 {
     static std::mutex m;
@@ -884,8 +951,8 @@ static int c2_launch(KernArgs & a, const C2Params & p, cudaStream_t stream)
         auto it = per_sm_cache.find({dev, (int)smem});
         if(it == per_sm_cache.end())
         {
-            cudaFuncSetAttribute(k_coop2<MODE, NT, DERIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop2<MODE, NT, DERIV>, NT, smem) != cudaSuccess)
+            cudaFuncSetAttribute(k_coop2<MODE, NT, DERIV, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop2<MODE, NT, DERIV, MIXED>, NT, smem) != cudaSuccess)
             {
                 cudaGetLastError();
                 per_sm = 1;
@@ -904,7 +971,7 @@ static int c2_launch(KernArgs & a, const C2Params & p, cudaStream_t stream)
         set_error("out of device memory for cooperative-kernel scratch");
         return SIMINT_B200_ERR_CUDA;
     }
-    k_coop2<MODE, NT, DERIV><<<(unsigned)grid, NT, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
+    k_coop2<MODE, NT, DERIV, MIXED><<<(unsigned)grid, NT, smem, stream>>>(a, p, (double *)w.dscratch.ptr);
     count_launch(1);
     return 0;
 }
@@ -942,20 +1009,27 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
     p.ordering = ordering();
     a.swapB = a.swapK = a.pq = 0;
     a.oidx = nullptr;
-    (void)prec;      // the VRR of this kernel runs in FP64 for both precision modes
+    // the FP32 VRR applies to deriv 0 in mixed mode with a positive gate
+    const bool mixed = prec == SIMINT_B200_PREC_MIXED && a.gate > 0.0 && deriv == 0;
     if(h->nthreads == 128)
     {
         if(deriv)
-            return mode == 0 ? c2_launch<0, 128, 1>(a, p, stream) : mode == 1 ? c2_launch<1, 128, 1>(a, p, stream)
-                                                                 : c2_launch<2, 128, 1>(a, p, stream);
-        return mode == 0 ? c2_launch<0, 128, 0>(a, p, stream) : mode == 1 ? c2_launch<1, 128, 0>(a, p, stream)
-                                                             : c2_launch<2, 128, 0>(a, p, stream);
+            return mode == 0 ? c2_launch<0, 128, 1, false>(a, p, stream)
+                 : mode == 1 ? c2_launch<1, 128, 1, false>(a, p, stream) : c2_launch<2, 128, 1, false>(a, p, stream);
+        if(mixed)
+            return mode == 0 ? c2_launch<0, 128, 0, true>(a, p, stream)
+                 : mode == 1 ? c2_launch<1, 128, 0, true>(a, p, stream) : c2_launch<2, 128, 0, true>(a, p, stream);
+        return mode == 0 ? c2_launch<0, 128, 0, false>(a, p, stream)
+             : mode == 1 ? c2_launch<1, 128, 0, false>(a, p, stream) : c2_launch<2, 128, 0, false>(a, p, stream);
     }
     if(deriv)
-        return mode == 0 ? c2_launch<0, 256, 1>(a, p, stream) : mode == 1 ? c2_launch<1, 256, 1>(a, p, stream)
-                                                             : c2_launch<2, 256, 1>(a, p, stream);
-    return mode == 0 ? c2_launch<0, 256, 0>(a, p, stream) : mode == 1 ? c2_launch<1, 256, 0>(a, p, stream)
-                                                         : c2_launch<2, 256, 0>(a, p, stream);
+        return mode == 0 ? c2_launch<0, 256, 1, false>(a, p, stream)
+             : mode == 1 ? c2_launch<1, 256, 1, false>(a, p, stream) : c2_launch<2, 256, 1, false>(a, p, stream);
+    if(mixed)
+        return mode == 0 ? c2_launch<0, 256, 0, true>(a, p, stream)
+             : mode == 1 ? c2_launch<1, 256, 0, true>(a, p, stream) : c2_launch<2, 256, 0, true>(a, p, stream);
+    return mode == 0 ? c2_launch<0, 256, 0, false>(a, p, stream)
+         : mode == 1 ? c2_launch<1, 256, 0, false>(a, p, stream) : c2_launch<2, 256, 0, false>(a, p, stream);
 }
 
 } // namespace sb200

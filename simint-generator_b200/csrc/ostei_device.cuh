@@ -65,6 +65,8 @@ struct QuartetCtx
     double bscreen_max;       // screen_max of the pair set in the bra role
     double kscreen_max;       // screen_max of the pair set in the ket role
     double gate;
+    int gL;                   // mixed precision: recursion depth L of the class
+    double gamp;              // mixed precision: HRR growth (1+|AB|)^nb (1+|CD|)^nd
     const unsigned short * oidx;
     const double * boys;
 };
@@ -252,9 +254,43 @@ __device__ __forceinline__ bool prim_setup(const QuartetCtx & c, const BraPrim &
     s.T = R2 * alpha;
     double pf = sqrt(one_over_sum);
     s.prefac = (bp.prefac * r[1]) * pf;
-    // mixed precision gate: Schwarz bound of this primitive quartet
-    s.lowprec = (bp.sq * r[15] < c.gate);
+    // mixed precision gate: estimated absolute error of an FP32 VRR for
+    // this primitive quartet.  Every (ss|ss)^(m) is at most |prefac|
+    // (F_m <= 1); a recursion step adds X and Y multiples of the level below
+    // and at most h = L (1/2p + 1/2q + 1/2(p+q)) times the level two below,
+    // so the largest value of level k is at most r^k |prefac| with r the
+    // root of r^2 = g r + h, g = 1 + max|X| + max|Y|; the HRR multiplies by
+    // at most gamp; FP32 rounding adds about 8 (L+1) units of 2^-24 relative
+    // to the largest intermediate.
+    s.lowprec = false;
+    if(c.gate > 0.0)
+    {
+        const double mx = fmax(fmax(fmax(fabs(s.PAx), fabs(s.PAy)), fmax(fabs(s.PAz), fabs(s.PBx))),
+                               fmax(fmax(fabs(s.PBy), fabs(s.PBz)), fmax(fabs(s.QCx), fabs(s.QCy))));
+        const double mq = fmax(fmax(fmax(fabs(s.QCz), fabs(s.QDx)), fabs(s.QDy)), fabs(s.QDz));
+        const double my = fmax(fmax(fmax(fabs(s.aopPQx), fabs(s.aopPQy)), fabs(s.aopPQz)),
+                               fmax(fmax(fabs(s.aoqPQx), fabs(s.aoqPQy)), fabs(s.aoqPQz)));
+        const double g = 1.0 + fmax(mx, mq) + my;
+        const double h = c.gL * (s.oo2p + s.oo2q + s.oo2pq);
+        const double r = 0.5 * (g + sqrt(fma(g, g, 4.0 * h)));
+        double est = fabs(s.prefac) * c.gamp * (8.0 * (c.gL + 1) * 5.9604644775390625e-08);
+        for(int k = 0; k < c.gL; k++)
+            est *= r;
+        s.lowprec = est < c.gate;
+    }
     return true;
+}
+
+// HRR growth factor of a shell quartet for the mixed-precision estimate:
+// the transfer multiplies by |AB| (|CD|) once per step, nb (nd) steps.
+__device__ __forceinline__ double hrr_amp(const QuartetCtx & c, int nb, int nd)
+{
+    const double ab = 1.0 + fmax(fmax(fabs(c.AB[0]), fabs(c.AB[1])), fabs(c.AB[2]));
+    const double cd = 1.0 + fmax(fmax(fabs(c.CD[0]), fabs(c.CD[1])), fabs(c.CD[2]));
+    double r = 1.0;
+    for(int k = 0; k < nb; k++) r *= ab;
+    for(int k = 0; k < nd; k++) r *= cd;
+    return r;
 }
 
 // Fill a QuartetCtx for requested bra pair iP and ket pair iQ.
@@ -279,6 +315,8 @@ __device__ __forceinline__ void make_ctx(const KernArgs & a, int iP, int iQ, Qua
     c.bscreen_max = B.screen_max;
     c.kscreen_max = K.screen_max;
     c.gate = a.gate;
+    c.gL = 0;
+    c.gamp = 1.0;
     c.oidx = a.oidx;
     c.boys = a.boys;
 }

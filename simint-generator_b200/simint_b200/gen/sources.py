@@ -42,6 +42,8 @@ def kernel_file(am):
     o.append("    if(!task_of<MODE>(a, t, iP, iQ, off)) return;")
     o.append("    QuartetCtx c;")
     o.append("    make_ctx(a, iP, iQ, c);")
+    o.append("    if(PREC == 1) { c.gL = %d; c.gamp = hrr_amp(c, %d, %d); }"
+             % (p.L, min(am[0], am[1]), min(am[2], am[3])))
     o.append("    if(PREC == 0) %s<false>(c, a.out + off);" % fn64)
     o.append("    else %s<true>(c, a.out + off);" % fnmx)
     o.append("}")
