@@ -244,17 +244,101 @@ __device__ __forceinline__ void c2_combo(const float * cf, int combo, float & X,
     X = q.x; Y = q.y; Z = q.z; O = q.w;
 }
 
-// The VRR of nb primitive quartets (prepared slots slot[0..nb)) in type T,
-// wavefront by wavefront, with the tops added to the FP64 accumulators in
-// slot order.  wave holds 3 wavefronts x cap batch entries x W values of T.
-template<typename T, int NT, int DERIV>
+// The wavefronts s >= 1 of NB primitive quartets (prepared slots
+// slot[0..NB)) in type T.  A thread takes units it = tid, tid + NT, ... of
+// each wavefront and runs each for all NB primitive quartets as independent
+// chains; the tops go to the FP64 accumulators in slot order.
+template<typename T, int NT, int DERIV, int NB>
+__device__ __forceinline__ void c2_waves(const C2Params & p, T * __restrict__ wave, int cap, int W,
+                                         const double * __restrict__ prep, int PS, int off32,
+                                         const int * __restrict__ slot, double * __restrict__ acc)
+{
+    const int tid = threadIdx.x;
+    const double * cfd[NB];
+    const T * cft[NB];
+    #pragma unroll
+    for(int bb = 0; bb < NB; bb++)
+    {
+        cfd[bb] = prep + slot[bb] * PS;
+        cft[bb] = (const T *)(cfd[bb] + off32);
+    }
+    for(int sf = 1; sf <= p.smax; sf++)
+    {
+        T * cur = wave + (sf % 3) * cap * W;
+        const T * w1 = wave + ((sf + 2) % 3) * cap * W;
+        const T * w2 = wave + ((sf + 1) % 3) * cap * W;
+        const int end = p.wstart[sf + 1];
+        for(int it = p.wstart[sf] + tid; it < end; it += NT)
+        {
+            const int4 q = __ldg(&p.items[it]);
+            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
+            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
+            const int acc0 = q.z & 0xffff;
+            const int combo = (q.z >> 16) & 7;
+            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
+            const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
+            T v[NB];
+            #pragma unroll
+            for(int bb = 0; bb < NB; bb++)
+            {
+                T X, Y, Z, O;
+                c2_combo(cft[bb], combo, X, Y, Z, O);
+                const T * s1 = w1 + bb * W + o1;
+                const T * s2 = w2 + bb * W + o2;
+                const T * s3 = w2 + bb * W + o3;
+                T r = X * s1[0];
+                r = fma(Y, s1[1], r);
+                if(has2)
+                    r = fma(dA * O, fma(Z, s2[1], s2[0]), r);
+                if(has3)
+                    r = fma(dB * cft[bb][K_O2PQ], s3[1], r);
+                v[bb] = r;
+            }
+            #pragma unroll
+            for(int bb = 0; bb < NB; bb++)
+                cur[bb * W + dsto] = v[bb];
+            // tops: added primitive quartet by primitive quartet, in order
+            if(acc0 != 0xffff)
+            {
+                double a = acc[acc0];
+                #pragma unroll
+                for(int bb = 0; bb < NB; bb++)
+                    a += (double)v[bb];
+                acc[acc0] = a;
+            }
+            if(DERIV)
+            {
+                const int tmask = ((q.z >> 26) & 15) << 1;
+                if(tmask)
+                {
+                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
+                    for(int tg = 1; tg < p.ntag; tg++)
+                        if((tmask >> tg) & 1)
+                        {
+                            const int re = gE - c2_lev_off(p.elo[tg]);
+                            const int rf = gF - c2_lev_off(p.flo[tg]);
+                            double & a = acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf];
+                            #pragma unroll
+                            for(int bb = 0; bb < NB; bb++)
+                                a += (double)v[bb] * cfd[bb][K_W1 + tg - 1];
+                        }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The VRR of nb primitive quartets (prepared slots slot[0..nb)) in type T:
+// block (0,0) from the Boys values, the (ss|ss) tops, then the wavefronts.
+// wave holds 3 wavefronts x cap batch entries x W values of T.
+template<typename T, int NT, int DERIV, int MAXB>
 __device__ __forceinline__ void c2_batch(const C2Params & p, T * __restrict__ wave, int cap, int W,
                                          const double * __restrict__ prep, int PS, int off32,
                                          const int * __restrict__ slot, int nb, double * __restrict__ acc)
 {
     const int tid = threadIdx.x;
     const int L = p.L;
-    // wavefront 0 = block (0,0), m = 0..L
     for(int k2 = tid; k2 < nb * (L + 1); k2 += NT)
     {
         const int bb = k2 / (L + 1), n = k2 - bb * (L + 1);
@@ -270,57 +354,16 @@ __device__ __forceinline__ void c2_batch(const C2Params & p, T * __restrict__ wa
                     acc[p.acc_off[tg]] += (tg == 0 ? 1.0 : cf[K_W1 + tg - 1]) * cf[C2_NCOEF];
         }
     __syncthreads();
-    for(int sf = 1; sf <= p.smax; sf++)
+    switch(nb)
     {
-        T * cur = wave + (sf % 3) * cap * W;
-        const T * w1 = wave + ((sf + 2) % 3) * cap * W;
-        const T * w2 = wave + ((sf + 1) % 3) * cap * W;
-        for(int it = p.wstart[sf] + tid; it < p.wstart[sf + 1]; it += NT)
-        {
-            const int4 q = __ldg(&p.items[it]);
-            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
-            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
-            const int acc0 = q.z & 0xffff;
-            const int combo = (q.z >> 16) & 7;
-            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
-            const int tmask = ((q.z >> 26) & 15) << 1;
-            const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
-            for(int bb = 0; bb < nb; bb++)
-            {
-                const double * cfd = prep + slot[bb] * PS;
-                const T * cf = (const T *)(cfd + off32);
-                T X, Y, Z, O;
-                c2_combo(cf, combo, X, Y, Z, O);
-                const T HA = dA * O;
-                const T HB = dB * cf[K_O2PQ];
-                const T * s1 = w1 + bb * W + o1;
-                const T * s2 = w2 + bb * W + o2;
-                const T * s3 = w2 + bb * W + o3;
-                T v = X * s1[0];
-                v = fma(Y, s1[1], v);
-                if(has2)
-                    v = fma(HA, fma(Z, s2[1], s2[0]), v);
-                if(has3)
-                    v = fma(HB, s3[1], v);
-                cur[bb * W + dsto] = v;
-                // tops: added primitive quartet by primitive quartet, in order
-                const double v0 = (double)v;
-                if(acc0 != 0xffff)
-                    acc[acc0] += v0;
-                if(DERIV && tmask)
-                {
-                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
-                    for(int tg = 1; tg < p.ntag; tg++)
-                        if((tmask >> tg) & 1)
-                        {
-                            const int re = gE - c2_lev_off(p.elo[tg]);
-                            const int rf = gF - c2_lev_off(p.flo[tg]);
-                            acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf] += v0 * cfd[K_W1 + tg - 1];
-                        }
-                }
-            }
-        }
-        __syncthreads();
+        case 1: c2_waves<T, NT, DERIV, 1>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 2: if constexpr(MAXB >= 2) c2_waves<T, NT, DERIV, 2>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 3: if constexpr(MAXB >= 3) c2_waves<T, NT, DERIV, 3>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 4: if constexpr(MAXB >= 4) c2_waves<T, NT, DERIV, 4>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 5: if constexpr(MAXB >= 5) c2_waves<T, NT, DERIV, 5>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 6: if constexpr(MAXB >= 6) c2_waves<T, NT, DERIV, 6>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        case 7: if constexpr(MAXB >= 7) c2_waves<T, NT, DERIV, 7>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
+        default: if constexpr(MAXB >= 8) c2_waves<T, NT, DERIV, 8>(p, wave, cap, W, prep, PS, off32, slot, acc); break;
     }
 }
 
@@ -463,11 +506,11 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
                 __syncthreads();
                 const int nhigh = MIXED ? s_nhigh : ng;
                 for(int b0 = 0; b0 < nhigh; b0 += B)
-                    c2_batch<double, NT, DERIV>(p, wave, B, W, prep, PS, 0, s_slot + b0, min(B, nhigh - b0), acc);
-                if(MIXED)
+                    c2_batch<double, NT, DERIV, 4>(p, wave, B, W, prep, PS, 0, s_slot + b0, min(B, nhigh - b0), acc);
+                if constexpr(MIXED)
                     for(int b0 = nhigh; b0 < ng; b0 += 2 * B)
-                        c2_batch<float, NT, DERIV>(p, (float *)wave, 2 * B, W, prep, PS, p.off32, s_slot + b0,
-                                                   min(2 * B, ng - b0), acc);
+                        c2_batch<float, NT, DERIV, 8>(p, (float *)wave, 2 * B, W, prep, PS, p.off32, s_slot + b0,
+                                                      min(2 * B, ng - b0), acc);
             }
             __syncthreads();      // surv, s_cnt and wcount are reused by the next chunk
         }
