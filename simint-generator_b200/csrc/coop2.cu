@@ -244,10 +244,78 @@ __device__ __forceinline__ void c2_combo(const float * cf, int combo, float & X,
     X = q.x; Y = q.y; Z = q.z; O = q.w;
 }
 
+// One VRR unit (one element, one auxiliary order) for NB primitive quartets.
+template<typename T, int NB>
+__device__ __forceinline__ void c2_unit(const int4 q, const T * __restrict__ w1, const T * __restrict__ w2,
+                                        int W, const T * const * cft, T * v)
+{
+    const int o1 = (int)((unsigned)q.x >> 16);
+    const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
+    const int combo = (q.z >> 16) & 7;
+    const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
+    const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
+    #pragma unroll
+    for(int bb = 0; bb < NB; bb++)
+    {
+        T X, Y, Z, O;
+        c2_combo(cft[bb], combo, X, Y, Z, O);
+        const T * s1 = w1 + bb * W + o1;
+        const T * s2 = w2 + bb * W + o2;
+        const T * s3 = w2 + bb * W + o3;
+        T r = X * s1[0];
+        r = fma(Y, s1[1], r);
+        if(has2)
+            r = fma(dA * O, fma(Z, s2[1], s2[0]), r);
+        if(has3)
+            r = fma(dB * cft[bb][K_O2PQ], s3[1], r);
+        v[bb] = r;
+    }
+}
+
+// Store a unit's NB results and add its tops to the FP64 accumulators in
+// primitive order.
+template<typename T, int NB, int DERIV>
+__device__ __forceinline__ void c2_unit_store(const C2Params & p, const int4 q, T * __restrict__ cur, int W,
+                                              const double * const * cfd, const T * v, double * __restrict__ acc)
+{
+    const int dsto = q.x & 0xffff;
+    #pragma unroll
+    for(int bb = 0; bb < NB; bb++)
+        cur[bb * W + dsto] = v[bb];
+    const int acc0 = q.z & 0xffff;
+    if(acc0 != 0xffff)
+    {
+        double a = acc[acc0];
+        #pragma unroll
+        for(int bb = 0; bb < NB; bb++)
+            a += (double)v[bb];
+        acc[acc0] = a;
+    }
+    if(DERIV)
+    {
+        const int tmask = ((q.z >> 26) & 15) << 1;
+        if(tmask)
+        {
+            const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
+            for(int tg = 1; tg < p.ntag; tg++)
+                if((tmask >> tg) & 1)
+                {
+                    const int re = gE - c2_lev_off(p.elo[tg]);
+                    const int rf = gF - c2_lev_off(p.flo[tg]);
+                    double & a = acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf];
+                    #pragma unroll
+                    for(int bb = 0; bb < NB; bb++)
+                        a += (double)v[bb] * cfd[bb][K_W1 + tg - 1];
+                }
+        }
+    }
+}
+
 // The wavefronts s >= 1 of NB primitive quartets (prepared slots
 // slot[0..NB)) in type T.  A thread takes units it = tid, tid + NT, ... of
-// each wavefront and runs each for all NB primitive quartets as independent
-// chains; the tops go to the FP64 accumulators in slot order.
+// each wavefront, two at a time, and runs each for all NB primitive
+// quartets as independent chains; the tops go to the FP64 accumulators in
+// slot order.
 template<typename T, int NT, int DERIV, int NB>
 __device__ __forceinline__ void c2_waves(const C2Params & p, T * __restrict__ wave, int cap, int W,
                                          const double * __restrict__ prep, int PS, int off32,
@@ -268,62 +336,17 @@ __device__ __forceinline__ void c2_waves(const C2Params & p, T * __restrict__ wa
         const T * w1 = wave + ((sf + 2) % 3) * cap * W;
         const T * w2 = wave + ((sf + 1) % 3) * cap * W;
         const int end = p.wstart[sf + 1];
-        for(int it = p.wstart[sf] + tid; it < end; it += NT)
+        for(int it = p.wstart[sf] + tid; it < end; it += 2 * NT)
         {
-            const int4 q = __ldg(&p.items[it]);
-            const int dsto = q.x & 0xffff, o1 = (int)((unsigned)q.x >> 16);
-            const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
-            const int acc0 = q.z & 0xffff;
-            const int combo = (q.z >> 16) & 7;
-            const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
-            const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
-            T v[NB];
-            #pragma unroll
-            for(int bb = 0; bb < NB; bb++)
-            {
-                T X, Y, Z, O;
-                c2_combo(cft[bb], combo, X, Y, Z, O);
-                const T * s1 = w1 + bb * W + o1;
-                const T * s2 = w2 + bb * W + o2;
-                const T * s3 = w2 + bb * W + o3;
-                T r = X * s1[0];
-                r = fma(Y, s1[1], r);
-                if(has2)
-                    r = fma(dA * O, fma(Z, s2[1], s2[0]), r);
-                if(has3)
-                    r = fma(dB * cft[bb][K_O2PQ], s3[1], r);
-                v[bb] = r;
-            }
-            #pragma unroll
-            for(int bb = 0; bb < NB; bb++)
-                cur[bb * W + dsto] = v[bb];
-            // tops: added primitive quartet by primitive quartet, in order
-            if(acc0 != 0xffff)
-            {
-                double a = acc[acc0];
-                #pragma unroll
-                for(int bb = 0; bb < NB; bb++)
-                    a += (double)v[bb];
-                acc[acc0] = a;
-            }
-            if(DERIV)
-            {
-                const int tmask = ((q.z >> 26) & 15) << 1;
-                if(tmask)
-                {
-                    const int gE = (q.w >> 8) & 1023, gF = (q.w >> 18) & 1023;
-                    for(int tg = 1; tg < p.ntag; tg++)
-                        if((tmask >> tg) & 1)
-                        {
-                            const int re = gE - c2_lev_off(p.elo[tg]);
-                            const int rf = gF - c2_lev_off(p.flo[tg]);
-                            double & a = acc[p.acc_off[tg] + re * p.acc_nf[tg] + rf];
-                            #pragma unroll
-                            for(int bb = 0; bb < NB; bb++)
-                                a += (double)v[bb] * cfd[bb][K_W1 + tg - 1];
-                        }
-                }
-            }
+            const bool two = it + NT < end;
+            const int4 q0 = __ldg(&p.items[it]);
+            const int4 q1 = two ? __ldg(&p.items[it + NT]) : q0;
+            T v0[NB], v1[NB];
+            c2_unit<T, NB>(q0, w1, w2, W, cft, v0);
+            c2_unit<T, NB>(q1, w1, w2, W, cft, v1);
+            c2_unit_store<T, NB, DERIV>(p, q0, cur, W, cfd, v0, acc);
+            if(two)
+                c2_unit_store<T, NB, DERIV>(p, q1, cur, W, cfd, v1, acc);
         }
         __syncthreads();
     }
