@@ -40,6 +40,20 @@ def _ensure_boys():
     return ensure_include(os.path.join(GEN, "boys_grid.inc"))
 
 
+def build_oracle_ld(force=False):
+    """oracle/liboracle_ld.so: the same restatement evaluated in long double
+    (-DORACLE_LONG_DOUBLE), used by the tests to measure the intrinsic
+    double-precision error of ill-conditioned elements."""
+    _ensure_boys()
+    out = os.path.join(HERE, "liboracle_ld.so")
+    src = os.path.join(HERE, "ostei_oracle.c")
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+        return out
+    _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-DORACLE_LONG_DOUBLE",
+          "-I", os.path.join(REPO, "include"), "-I", GEN, "-o", out, src, "-lm"])
+    return out
+
+
 def build_oracle(force=False):
     _ensure_boys()
     out = os.path.join(HERE, "liboracle.so")

@@ -45,6 +45,19 @@ def load_oracle():
     return lib
 
 
+def load_oracle_ld():
+    """The oracle evaluated in long double (same pairs, same algorithm);
+    oracle_compute_eri writes long double values."""
+    path = os.path.join(HERE, "liboracle_ld.so")
+    if not os.path.exists(path):
+        from build import build_oracle_ld  # noqa
+        build_oracle_ld()
+    lib = C.CDLL(path)
+    lib.oracle_compute_eri.argtypes = [PairP, PairP, C.c_double, C.c_int, C.c_int, C.c_void_p]
+    lib.oracle_compute_eri.restype = C.c_int
+    return lib
+
+
 def load_ref():
     """The reference-built library, or None when it was not built here."""
     path = os.path.join(HERE, "_ref", "libsimint_ref.so")

@@ -49,6 +49,26 @@
 #include "simint/shell/shell.h"
 #include "boys_grid.inc"
 
+/* Arithmetic type of the integral evaluation (pair data, shells and
+ * screening values stay double).  The oracle is built twice: double, and
+ * with -DORACLE_LONG_DOUBLE long double -- the same algorithm evaluated with
+ * 64-bit mantissas, which measures how far any double-precision evaluation
+ * (this oracle's or the product's) is from the exact values on elements that
+ * the recurrences compute with cancellation. */
+#ifdef ORACLE_LONG_DOUBLE
+typedef long double real;
+#define R_EXP expl
+#define R_SQRT sqrtl
+#define R_POW powl
+#define R_FMA fmal
+#else
+typedef double real;
+#define R_EXP exp
+#define R_SQRT sqrt
+#define R_POW pow
+#define R_FMA fma
+#endif
+
 #define NC(l) ((l) >= 0 ? (((l) + 1) * ((l) + 2)) / 2 : 0)
 #define MAXLEV 24                       /* largest AM level handled */
 #define SQRT_TWO_PI_52 5.91496717279561287782347843505365022963403204272156069835237
@@ -122,18 +142,18 @@ static int stepdir(const int g[3])
 /* Boys function                                                       */
 /* ------------------------------------------------------------------ */
 
-static double taylor_single(double x, int n)
+static real taylor_single(real x, int n)
 {
     const int idx = (int)(10.0 * (x + 0.05));
-    const double xi = (double)idx * 0.1;
-    const double dx = xi - x;
+    const real xi = (real)idx * 0.1;
+    const real dx = xi - x;
     const double * g = &simint_b200_boys_grid_host[idx][n];
     return g[0] + dx * (g[1] + dx * ((1.0/2.0) * g[2] + dx * ((1.0/6.0) * g[3]
            + dx * ((1.0/24.0) * g[4] + dx * ((1.0/120.0) * g[5]
            + dx * ((1.0/720.0) * g[6] + dx * ((1.0/5040.0) * g[7])))))));
 }
 
-void oracle_boys(double x, int L, double * F)
+void oracle_boys(real x, int L, real * F)
 {
     if(L < 4)
     {
@@ -144,8 +164,8 @@ void oracle_boys(double x, int L, double * F)
         }
         else
         {
-            const double x1 = 1.0 / x;
-            double x2 = sqrt(x1);
+            const real x1 = 1.0 / x;
+            real x2 = R_SQRT(x1);
             for(int n = 0; n <= L; n++)
             {
                 F[n] = simint_b200_boys_longfac_host[n] * x2;
@@ -157,11 +177,11 @@ void oracle_boys(double x, int L, double * F)
     if(x < SIMINT_B200_BOYS_MAXX)
         F[L] = taylor_single(x, L);
     else
-        F[L] = simint_b200_boys_longfac_host[L] * pow(x, -((double)L + 0.5));
-    const double x2 = 2.0 * x;
-    const double ex = exp(-x);
+        F[L] = simint_b200_boys_longfac_host[L] * R_POW(x, -((real)L + 0.5));
+    const real x2 = 2.0 * x;
+    const real ex = R_EXP(-x);
     for(int n = L - 1; n >= 0; n--)
-        F[n] = (1.0 / (2.0 * n + 1)) * fma(x2, F[n + 1], ex);
+        F[n] = (1.0 / (2.0 * n + 1)) * R_FMA(x2, F[n + 1], ex);
 }
 
 /* ------------------------------------------------------------------ */
@@ -198,7 +218,7 @@ static int round8(int x) { return (x + 7) & ~7; }
 
 int oracle_compute_eri(struct simint_multi_shellpair const * P,
                        struct simint_multi_shellpair const * Q,
-                       double screen_tol, int deriv, int ordering, double * out);
+                       double screen_tol, int deriv, int ordering, real * out);
 
 static double prim_schwarz_one(const struct simint_shell * A, int i,
                                const struct simint_shell * B, int j);
@@ -369,13 +389,13 @@ static double prim_schwarz_one(const struct simint_shell * A, int i,
     struct simint_multi_shellpair P;
     oracle_create_pair(1, sh, &P, 0);
     const int n1 = NC(A->am), n2 = NC(B->am), n12 = n1 * n2;
-    double * ints = (double *)malloc(sizeof(double) * n12 * n12);
+    real * ints = (real *)malloc(sizeof(real) * n12 * n12);
     oracle_compute_eri(&P, &P, 0.0, 0, 0, ints);
     double mx = 0.0;
     for(int m = 0; m < n1; m++)
         for(int n = 0; n < n2; n++)
         {
-            const double v = fabs(ints[m * n2 * n1 * n2 + m * n2 + n * n1 * n2 + n]);
+            const double v = fabs((double)ints[m * n2 * n1 * n2 + m * n2 + n * n1 * n2 + n]);
             if(v > mx) mx = v;
         }
     free(ints);
@@ -389,11 +409,11 @@ double oracle_shellscreen_schwarz(const struct simint_shell * A, const struct si
     struct simint_multi_shellpair P;
     oracle_create_pair(1, sh, &P, 0);
     const int n12 = NC(A->am) * NC(B->am);
-    double * ints = (double *)malloc(sizeof(double) * n12 * n12);
+    real * ints = (real *)malloc(sizeof(real) * n12 * n12);
     oracle_compute_eri(&P, &P, 0.0, 0, 0, ints);
     double mx = 0.0;
     for(int n = 0; n < n12 * n12; n++)
-        if(fabs(ints[n]) > mx) mx = fabs(ints[n]);
+        if(fabs((double)ints[n]) > mx) mx = fabs((double)ints[n]);
     free(ints);
     oracle_free_pair(&P);
     return mx;
@@ -481,16 +501,16 @@ static void class_setup(const int am[4], int deriv, ClassInfo * ci)
 
 typedef struct
 {
-    double XP[3];      /* PA or PB, for the bra top centre */
-    double XQ[3];      /* QC or QD, for the ket top centre */
-    double aop_PQ[3], aoq_PQ[3];
-    double a_over_p, a_over_q;         /* both negative, as in the reference */
-    double one_over_2p, one_over_2q, one_over_2pq;
+    real XP[3];      /* PA or PB, for the bra top centre */
+    real XQ[3];      /* QC or QD, for the ket top centre */
+    real aop_PQ[3], aoq_PQ[3];
+    real a_over_p, a_over_q;         /* both negative, as in the reference */
+    real one_over_2p, one_over_2q, one_over_2pq;
 } PrimFactors;
 
 /* V[(gE * nF + gF) * (L+1) + m] */
-static void dense_vrr(const ClassInfo * ci, const PrimFactors * f, const double * F,
-                      double * V, int nE, int nF)
+static void dense_vrr(const ClassInfo * ci, const PrimFactors * f, const real * F,
+                      real * V, int nE, int nF)
 {
     const int L = ci->L;
     const int LP = L + 1;
@@ -525,16 +545,16 @@ static void dense_vrr(const ClassInfo * ci, const PrimFactors * f, const double 
                         const int have6 = e1[x] >= 0;
                         const int gF2 = have2 ? gidx(f2) : 0;
                         const int gE1 = have6 ? gidx(e1) : 0;
-                        const double c0 = (gf[x] - 1) == 1 ? f->one_over_2q : (double)(gf[x] - 1) * f->one_over_2q;
-                        const double c2 = ge[x] == 1 ? f->one_over_2pq : (double)ge[x] * f->one_over_2pq;
+                        const real c0 = (gf[x] - 1) == 1 ? f->one_over_2q : (real)(gf[x] - 1) * f->one_over_2q;
+                        const real c2 = ge[x] == 1 ? f->one_over_2pq : (real)ge[x] * f->one_over_2pq;
                         for(int m = 0; m <= mmax; m++)
                         {
-                            double t = f->XQ[x] * VV(gE, gF1, m);
-                            t = fma(f->aoq_PQ[x], VV(gE, gF1, m + 1), t);
+                            real t = f->XQ[x] * VV(gE, gF1, m);
+                            t = R_FMA(f->aoq_PQ[x], VV(gE, gF1, m + 1), t);
                             if(have2)
-                                t = fma(c0, fma(f->a_over_q, VV(gE, gF2, m + 1), VV(gE, gF2, m)), t);
+                                t = R_FMA(c0, R_FMA(f->a_over_q, VV(gE, gF2, m + 1), VV(gE, gF2, m)), t);
                             if(have6)
-                                t = fma(c2, VV(gE1, gF1, m + 1), t);
+                                t = R_FMA(c2, VV(gE1, gF1, m + 1), t);
                             VV(gE, gF, m) = t;
                         }
                     }
@@ -549,16 +569,16 @@ static void dense_vrr(const ClassInfo * ci, const PrimFactors * f, const double 
                         const int have6 = f1[x] >= 0;
                         const int gE2 = have2 ? gidx(e2) : 0;
                         const int gF1 = have6 ? gidx(f1) : 0;
-                        const double c0 = (ge[x] - 1) == 1 ? f->one_over_2p : (double)(ge[x] - 1) * f->one_over_2p;
-                        const double c2 = gf[x] == 1 ? f->one_over_2pq : (double)gf[x] * f->one_over_2pq;
+                        const real c0 = (ge[x] - 1) == 1 ? f->one_over_2p : (real)(ge[x] - 1) * f->one_over_2p;
+                        const real c2 = gf[x] == 1 ? f->one_over_2pq : (real)gf[x] * f->one_over_2pq;
                         for(int m = 0; m <= mmax; m++)
                         {
-                            double t = f->XP[x] * VV(gE1, gF, m);
-                            t = fma(f->aop_PQ[x], VV(gE1, gF, m + 1), t);
+                            real t = f->XP[x] * VV(gE1, gF, m);
+                            t = R_FMA(f->aop_PQ[x], VV(gE1, gF, m + 1), t);
                             if(have2)
-                                t = fma(c0, fma(f->a_over_p, VV(gE2, gF, m + 1), VV(gE2, gF, m)), t);
+                                t = R_FMA(c0, R_FMA(f->a_over_p, VV(gE2, gF, m + 1), VV(gE2, gF, m)), t);
                             if(have6)
-                                t = fma(c2, VV(gE1, gF1, m + 1), t);
+                                t = R_FMA(c2, VV(gE1, gF1, m + 1), t);
                             VV(gE, gF, m) = t;
                         }
                     }
@@ -576,13 +596,13 @@ static void dense_vrr(const ClassInfo * ci, const PrimFactors * f, const double 
  * (levels up to ta+tb).  right_step: 1 for I->J / K->L (tops (e,0), step on
  * the right function), 0 for J->I / L->K (tops (0,e), step on the left).
  * out[(psi4(A)*NC(tb) + psi4(B)) * ncol + col]. */
-static void hrr_side(int right_step, int ta, int tb, const double X[3],
-                     const double * top, int ncol, double * out)
+static void hrr_side(int right_step, int ta, int tb, const real X[3],
+                     const real * top, int ncol, real * out)
 {
     const int lt = ta + tb;
     const int nall = lev_off(lt + 1);
     const int nstep = right_step ? lev_off(tb + 1) : lev_off(ta + 1);
-    double * H = (double *)malloc(sizeof(double) * (size_t)nall * nstep * ncol);
+    real * H = (real *)malloc(sizeof(real) * (size_t)nall * nstep * ncol);
     int cs[MAXLEV * MAXLEV][3], co[MAXLEV * MAXLEV][3];
 #define HH(gt, gs, c) H[((size_t)(gt) * nstep + (gs)) * ncol + (c)]
     /* H(gt, gs): gt indexes the function on the top centre, gs the one that
@@ -612,9 +632,9 @@ static void hrr_side(int right_step, int ta, int tb, const double X[3],
                     for(int c = 0; c < ncol; c++)
                     {
                         if(right_step)   /* (a,b) = (a+1x, b-1x) + X (a, b-1x) */
-                            HH(it, is, c) = fma(X[x], HH(it, ism, c), HH(itp, ism, c));
+                            HH(it, is, c) = R_FMA(X[x], HH(it, ism, c), HH(itp, ism, c));
                         else             /* (a,b) = (a-1x, b+1x) - X (a-1x, b) */
-                            HH(it, is, c) = fma(-X[x], HH(it, ism, c), HH(itp, ism, c));
+                            HH(it, is, c) = R_FMA(-X[x], HH(it, ism, c), HH(itp, ism, c));
                     }
                 }
         }
@@ -636,8 +656,8 @@ static void hrr_side(int right_step, int ta, int tb, const double X[3],
 }
 
 /* full HRR: Acc[gE * nF + gF] -> target (ta tb | tc td), Psi4 order */
-static void hrr_full(const ClassInfo * ci, const int t[4], const double AB[3], const double CD[3],
-                     const double * Acc, int nE, int nF, double * out)
+static void hrr_full(const ClassInfo * ci, const int t[4], const real AB[3], const real CD[3],
+                     const real * Acc, int nE, int nF, real * out)
 {
     const int fl_lo = ci->ketstep_l ? t[2] : t[3];
     const int fl_hi = t[2] + t[3];
@@ -645,19 +665,19 @@ static void hrr_full(const ClassInfo * ci, const int t[4], const double AB[3], c
     (void)fl_lo;
     /* bra HRR for every ket column gF < ncolF */
     const int nbra = NC(t[0]) * NC(t[1]);
-    double * top = (double *)malloc(sizeof(double) * (size_t)nE * ncolF);
+    real * top = (real *)malloc(sizeof(real) * (size_t)nE * ncolF);
     for(int e = 0; e < nE; e++)
         for(int f = 0; f < ncolF; f++)
             top[(size_t)e * ncolF + f] = Acc[(size_t)e * nF + f];
-    double * bra = (double *)malloc(sizeof(double) * (size_t)nbra * ncolF);
+    real * bra = (real *)malloc(sizeof(real) * (size_t)nbra * ncolF);
     hrr_side(ci->brastep_j, t[0], t[1], AB, top, ncolF, bra);
     /* ket HRR: columns are the bra Cartesians */
-    double * top2 = (double *)malloc(sizeof(double) * (size_t)ncolF * nbra);
+    real * top2 = (real *)malloc(sizeof(real) * (size_t)ncolF * nbra);
     for(int f = 0; f < ncolF; f++)
         for(int b = 0; b < nbra; b++)
             top2[(size_t)f * nbra + b] = bra[(size_t)b * ncolF + f];
     const int nket = NC(t[2]) * NC(t[3]);
-    double * ket = (double *)malloc(sizeof(double) * (size_t)nket * nbra);
+    real * ket = (real *)malloc(sizeof(real) * (size_t)nket * nbra);
     hrr_side(ci->ketstep_l, t[2], t[3], CD, top2, nbra, ket);
     for(int b = 0; b < nbra; b++)
         for(int k = 0; k < nket; k++)
@@ -683,7 +703,7 @@ static void pair_offsets(const struct simint_multi_shellpair * P, int * start)
 
 int oracle_compute_eri(struct simint_multi_shellpair const * P,
                        struct simint_multi_shellpair const * Q,
-                       double screen_tol, int deriv, int ordering, double * out)
+                       double screen_tol, int deriv, int ordering, real * out)
 {
     const double tol2 = screen_tol * screen_tol;
     if(screen_tol > 0.0 && P->screen_max * Q->screen_max < tol2)
@@ -694,28 +714,28 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
     class_setup(am, deriv, &ci);
     const int nE = lev_off(ci.Emax + 1), nF = lev_off(ci.Fmax + 1);
     const int LP = ci.L + 1;
-    double * V = (double *)malloc(sizeof(double) * (size_t)nE * nF * LP);
-    double * Acc = (double *)malloc(sizeof(double) * 5 * (size_t)nE * nF);
+    real * V = (real *)malloc(sizeof(real) * (size_t)nE * nF * LP);
+    real * Acc = (real *)malloc(sizeof(real) * 5 * (size_t)nE * nF);
     const int ncart = NC(am[0]) * NC(am[1]) * NC(am[2]) * NC(am[3]);
     const int nout = ncart * (deriv ? 12 : 1);
-    double * tmp = (double *)malloc(sizeof(double) * 8 * (size_t)lev_off(ci.Emax + 2) * lev_off(ci.Fmax + 2));
-    double * res[8];
+    real * tmp = (real *)malloc(sizeof(real) * 8 * (size_t)lev_off(ci.Emax + 2) * lev_off(ci.Fmax + 2));
+    real * res[8];
     for(int t = 0; t < ci.ntarget; t++)
     {
         const int n = NC(ci.tgt[t][0]) * NC(ci.tgt[t][1]) * NC(ci.tgt[t][2]) * NC(ci.tgt[t][3]);
-        res[t] = (double *)malloc(sizeof(double) * (size_t)n);
+        res[t] = (real *)malloc(sizeof(real) * (size_t)n);
     }
     int * pst = (int *)malloc(sizeof(int) * (P->nshell12 + 1));
     int * qst = (int *)malloc(sizeof(int) * (Q->nshell12 + 1));
     pair_offsets(P, pst);
     pair_offsets(Q, qst);
-    double F[64];
+    real F[64];
     const int bra_on_A = ci.brastep_j, ket_on_C = ci.ketstep_l;
 
     for(int ab = 0; ab < P->nshell12_clip; ab++)
     for(int cd = 0; cd < Q->nshell12_clip; cd++)
     {
-        memset(Acc, 0, sizeof(double) * 5 * (size_t)nE * nF);
+        memset(Acc, 0, sizeof(real) * 5 * (size_t)nE * nF);
         for(int i = pst[ab]; i < pst[ab] + P->nprim12[ab]; i++)
         {
             if(check && P->screen[i] * Q->screen_max < tol2)
@@ -734,20 +754,20 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                     }
                     if(vmax < tol2) continue;
                 }
-                const double pa = P->alpha[i], qa = Q->alpha[j];
-                const double one_over_sum = 1.0 / (pa + qa);
-                const double PQ[3] = {P->x[i] - Q->x[j], P->y[i] - Q->y[j], P->z[i] - Q->z[j]};
-                double R2 = PQ[0] * PQ[0];
-                R2 = fma(PQ[1], PQ[1], R2);
-                R2 = fma(PQ[2], PQ[2], R2);
-                const double alpha = (pa * qa) * one_over_sum;
+                const real pa = P->alpha[i], qa = Q->alpha[j];
+                const real one_over_sum = 1.0 / (pa + qa);
+                const real PQ[3] = {P->x[i] - Q->x[j], P->y[i] - Q->y[j], P->z[i] - Q->z[j]};
+                real R2 = PQ[0] * PQ[0];
+                R2 = R_FMA(PQ[1], PQ[1], R2);
+                R2 = R_FMA(PQ[2], PQ[2], R2);
+                const real alpha = (pa * qa) * one_over_sum;
                 PrimFactors f;
-                const double one_over_p = 1.0 / pa, one_over_q = 1.0 / qa;
+                const real one_over_p = 1.0 / pa, one_over_q = 1.0 / qa;
                 f.one_over_2p = 0.5 * one_over_p;
                 f.one_over_2q = 0.5 * one_over_q;
                 f.one_over_2pq = 0.5 * one_over_sum;
                 f.a_over_p = -alpha * one_over_p;
-                const double aoq = alpha * one_over_q;
+                const real aoq = alpha * one_over_q;
                 f.a_over_q = -aoq;
                 for(int k = 0; k < 3; k++)
                 {
@@ -759,14 +779,14 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                 if(ket_on_C) { f.XQ[0] = Q->PA_x[j]; f.XQ[1] = Q->PA_y[j]; f.XQ[2] = Q->PA_z[j]; }
                 else         { f.XQ[0] = Q->PB_x[j]; f.XQ[1] = Q->PB_y[j]; f.XQ[2] = Q->PB_z[j]; }
                 oracle_boys(R2 * alpha, ci.L, F);
-                double prefac = sqrt(one_over_sum);
+                real prefac = R_SQRT(one_over_sum);
                 prefac = (P->prefac[i] * Q->prefac[j]) * prefac;
                 for(int n = 0; n <= ci.L; n++) F[n] *= prefac;
                 dense_vrr(&ci, &f, F, V, nE, nF);
-                const double w[5] = {1.0, P->alpha2[i], P->beta2[i], Q->alpha2[j], Q->beta2[j]};
+                const real w[5] = {1.0, P->alpha2[i], P->beta2[i], Q->alpha2[j], Q->beta2[j]};
                 for(int tg = 0; tg < (deriv ? 5 : 1); tg++)
                 {
-                    double * A = Acc + (size_t)tg * nE * nF;
+                    real * A = Acc + (size_t)tg * nE * nF;
                     for(int e = 0; e < nE; e++)
                         for(int g = 0; g < nF; g++)
                             A[(size_t)e * nF + g] += (tg == 0) ? V[((size_t)e * nF + g) * LP]
@@ -774,12 +794,12 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                 }
             }
         }
-        const double AB[3] = {P->AB_x[ab], P->AB_y[ab], P->AB_z[ab]};
-        const double CD[3] = {Q->AB_x[cd], Q->AB_y[cd], Q->AB_z[cd]};
+        const real AB[3] = {P->AB_x[ab], P->AB_y[ab], P->AB_z[ab]};
+        const real CD[3] = {Q->AB_x[cd], Q->AB_y[cd], Q->AB_z[cd]};
         for(int t = 0; t < ci.ntarget; t++)
             hrr_full(&ci, ci.tgt[t], AB, CD, Acc + (size_t)ci.tgt_tag[t] * nE * nF, nE, nF, res[t]);
 
-        double * o = out + ((size_t)ab * Q->nshell12_clip + cd) * nout;
+        real * o = out + ((size_t)ab * Q->nshell12_clip + cd) * nout;
         int ca[MAXLEV * MAXLEV][3], cb[MAXLEV * MAXLEV][3], cc[MAXLEV * MAXLEV][3], cdd[MAXLEV * MAXLEV][3];
         level_carts(am[0], ca); level_carts(am[1], cb); level_carts(am[2], cc); level_carts(am[3], cdd);
         for(int a = 0; a < NC(am[0]); a++)
@@ -794,7 +814,7 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                 o[oi] = res[0][((a * NC(am[1]) + b) * NC(am[2]) + c) * NC(am[3]) + d];
                 continue;
             }
-            double g12[12];
+            real g12[12];
             const int * gg[4] = {ca[a], cb[b], cc[c], cdd[d]};
             for(int t = 0; t < ci.ntarget; t++)
             {
@@ -821,7 +841,7 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                     const int * tt = ci.tgt[tp];
                     int idx = ((psi4_index(g[0][0], g[0][1], g[0][2]) * NC(tt[1]) + psi4_index(g[1][0], g[1][1], g[1][2])) * NC(tt[2])
                                + psi4_index(g[2][0], g[2][1], g[2][2])) * NC(tt[3]) + psi4_index(g[3][0], g[3][1], g[3][2]);
-                    double v = res[tp][idx];
+                    real v = res[tp][idx];
                     if(gg[ctr][x] > 0)
                     {
                         g[ctr][x] -= 2;
@@ -836,7 +856,7 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
             const int ms = ci.missing;
             for(int x = 0; x < 3; x++)
             {
-                double s = 0.0;
+                real s = 0.0;
                 int first = 1;
                 for(int ctr = 0; ctr < 4; ctr++)
                 {

@@ -44,3 +44,21 @@ def oracle_eri(orc, P, Q, tol=0.0, deriv=0, ordering=0):
     r = orc.oracle_compute_eri(C.byref(P), C.byref(Q), tol, deriv, ordering,
                                out.ctypes.data_as(C.POINTER(C.c_double)))
     return r, out
+
+
+def oracle_eri_ld(orc_ld, P, Q, tol=0.0, deriv=0, ordering=0):
+    """The same integrals from the long-double build of the oracle."""
+    n = P.nshell12_clip * Q.nshell12_clip * NC(P.am1) * NC(P.am2) * NC(Q.am1) * NC(Q.am2)
+    out = np.zeros(n * (12 if deriv else 1), dtype=np.longdouble)
+    r = orc_ld.oracle_compute_eri(C.byref(P), C.byref(Q), tol, deriv, ordering, out.ctypes.data)
+    return r, out
+
+
+def as_accurate_as_oracle(calc, ref, ref_ld, slack=2.0, floor=1e-14):
+    """Indices where calc is further from the long-double values than
+    slack x the double-precision oracle's largest error over the same block
+    (plus floor): the elements on which calc is less accurate than the
+    reference algorithm evaluated in double."""
+    e_calc = np.abs(calc.astype(np.longdouble) - ref_ld)
+    e_ref = float(np.abs(ref.astype(np.longdouble) - ref_ld).max()) if ref.size else 0.0
+    return np.nonzero(e_calc > slack * e_ref + floor)[0]

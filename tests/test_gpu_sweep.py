@@ -4,8 +4,13 @@ A small basis (s..g shells on a few pseudo-atoms) is swept in full-layout
 mode.  For every class the oracle computes the whole bra-class x ket-class
 rectangle from pair lists built exactly like the sweep's (same pairs, same
 order, same primitive Schwarz screening), and every quartet the sweep kept
-is compared with it.  Checksums must equal sums over the output; graph
-replay and streaming through a small buffer must reproduce them."""
+is compared with it (bar: abs 1e-13 or rel 1e-11; a quartet with elements
+outside it passes only if none of its elements is further from the
+long-double evaluation of the same algorithm than twice the double-precision
+oracle's largest error on that quartet, i.e. the gap is the intrinsic error
+of the recurrences in double).  Checksums must equal sums over the
+output; graph replay and streaming through a small buffer must reproduce
+them."""
 import ctypes as C
 
 import numpy as np
@@ -14,8 +19,8 @@ import pytest
 import simint_b200 as sb
 from simint_b200.capi import ShellSet
 from simint_b200.workloads import random_shells
-from oracle import load_oracle
-from _util import oracle_pairs, oracle_eri, parity_bad, NC
+from oracle import load_oracle, load_oracle_ld
+from _util import oracle_pairs, oracle_eri, oracle_eri_ld, parity_bad, as_accurate_as_oracle, NC
 
 pytestmark = pytest.mark.gpu
 
@@ -26,12 +31,13 @@ def setup():
     lib = sb.load()
     lib.simint_init()
     orc = load_oracle()
+    orc_ld = load_oracle_ld()
     rng = np.random.default_rng(2024)
     shells = random_shells(rng, [0, 0, 1, 1, 2, 3, 0, 1, 2, 0, 1, 4], nprim_range=(1, 4),
                            alpha=(0.1, 300.0), box=6.0, natom=4)
     S = ShellSet(shells)
     lib.simint_normalize_shells(S.n, S.ptr(0))
-    return torch, lib, orc, S, [s[0] for s in shells]
+    return torch, lib, orc, orc_ld, S, [s[0] for s in shells]
 
 
 def pair_class_list(ams, la, lb):
@@ -43,7 +49,7 @@ def pair_class_list(ams, la, lb):
 @pytest.mark.parametrize("tol", [0.0, 1e-12])
 @pytest.mark.parametrize("ordering", [0, 1])
 def test_sweep_matches_oracle(setup, tol, ordering):
-    torch, lib, orc, S, ams = setup
+    torch, lib, orc, orc_ld, S, ams = setup
     lib.simint_b200_set_ordering(ordering)
     B = sb.Basis(S, tol, max_am=4, lib=lib)
     n = B.output_size
@@ -74,7 +80,19 @@ def test_sweep_matches_oracle(setup, tol, ordering):
             want = ref[bidx[(a, b)], kidx[(cc, d)]]
             got = blk[q * c["nout"]:(q + 1) * c["nout"]]
             bad, dmax = parity_bad(got, want)
-            assert len(bad) == 0, (c["am"], q, dmax, got[bad[:4]], want[bad[:4]], np.abs(want).max())
+            if len(bad):
+                # elements outside the abs/rel bar: the recurrences compute them
+                # with cancellation, so every double-precision evaluation has
+                # errors of that size; accept them only where the product is as
+                # close to the long-double evaluation as the oracle is
+                P1 = oracle_pairs(orc, S, [(a, b)], screen)
+                Q1 = oracle_pairs(orc, S, [(cc, d)], screen)
+                _, want_ld = oracle_eri_ld(orc_ld, P1, Q1, tol, 0, ordering)
+                orc.oracle_free_pair(C.byref(P1))
+                orc.oracle_free_pair(C.byref(Q1))
+                worse = as_accurate_as_oracle(got, want, want_ld)
+                assert len(worse) == 0, (c["am"], q, dmax, got[worse[:4]], want[worse[:4]],
+                                         np.abs(want).max())
     # graph replay gives the same checksums
     B.compute(sb.FP64, out.data_ptr(), n)
     B.compute(sb.FP64, out.data_ptr(), n)

@@ -168,3 +168,29 @@ def test_library_pairs_match_reference_shell_c(name):
     if screen:
         np.testing.assert_allclose(a["screen"], PAIRS[name + "/screen"], rtol=1e-15)
     lib.simint_free_multi_shellpair(C.byref(P))
+
+
+@pytest.mark.parametrize("key", _classes(D0)[::4])
+def test_long_double_oracle_against_valeevref(orc, key):
+    """The long-double build of the oracle (used to measure the intrinsic
+    double-precision error of cancelling elements) is at least as close to
+    ValeevRef (the reference's long-double oracle) as the double build."""
+    from oracle import load_oracle_ld
+    from _util import oracle_eri_ld
+    orc_ld = load_oracle_ld()
+    shells = _shells(D0, key)
+    nsh = [int(x) for x in D0[key + "/nsh"]]
+    S = ShellSet(shells)
+    idx = np.cumsum([0] + nsh)
+    grp = [list(range(idx[k], idx[k + 1])) for k in range(4)]
+    P = oracle_pairs(orc, S, [(i, j) for i in grp[0] for j in grp[1]])
+    Q = oracle_pairs(orc, S, [(i, j) for i in grp[2] for j in grp[3]])
+    _, out = oracle_eri(orc, P, Q, 0.0, 0, 0)
+    _, out_ld = oracle_eri_ld(orc_ld, P, Q, 0.0, 0, 0)
+    orc.oracle_free_pair(C.byref(P))
+    orc.oracle_free_pair(C.byref(Q))
+    ref = D0[key + "/values"].astype(np.longdouble)
+    e64 = float(np.abs(out - ref).max())
+    eld = float(np.abs(out_ld - ref).max())
+    scale = float(np.abs(ref).max())
+    assert eld <= e64 + 2e-16 * scale, (key, eld, e64)
