@@ -344,13 +344,15 @@ def run_b200(args):
     dc = classes[dom]
     dom_fl = flops_of_class(dc["am"], dc["nprimq"], dc["nquart"])
     achieved = dom_fl / (ctmx[dom] / 1e3) / 1e12
+    # DRAM bytes of the dominant class's launch: bytes per shell quartet from
+    # one ncu capture of that kernel (profiles/traffic.json) times the
+    # quartets this launch processes (traffic grows with the output)
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("".join("spdfg"[x] for x in dc["am"]))
-        except Exception:
-            traffic = None
+        ent = json.load(open(prof)).get("".join("spdfg"[x] for x in dc["am"]))
+        if ent:
+            traffic = ent["dram_bytes_per_quartet"] * dc["nquart"]
 
     # e2e through the reference-facing C ABI, host buffers
     e2e = None
