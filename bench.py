@@ -410,7 +410,8 @@ def run_b200(args):
             "roofline": {"bound": "fp64", "kernel": "class " + "".join("spdfg"[x] for x in dc["am"]),
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 > 0 else None, "traffic": traffic,
-                         "peak_source": "measured FMA-chain probe (simint_b200_fma_peak)",
+                         "peak_source": "measured FP64 FMA-chain probe (simint_b200_fma_peak), of measured",
+                         "flop_model": "reference generator op counts per unique class (simint_b200.perfmodel)",
                          "fp32_peak": peak32},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clkmx, "clocks_fp64": clk64, "per_class": per_class,
