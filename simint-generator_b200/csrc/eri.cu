@@ -212,11 +212,15 @@ void init_tables()
 // Per-thread device workspace (grow-only)
 // ---------------------------------------------------------------------
 
+static thread_local Workspace * t_ws_override = nullptr;
+
 Workspace & workspace()
 {
     static thread_local Workspace w;
-    return w;
+    return t_ws_override ? *t_ws_override : w;
 }
+
+void set_workspace_override(Workspace * w) { t_ws_override = w; }
 
 bool DevBuf::reserve(size_t n)
 {

@@ -57,6 +57,9 @@ int ordering();
 int precision();
 double gate();
 Workspace & workspace();
+// Launches issued by this host thread use `w` (nullptr: the thread's own
+// workspace) for their scratch: concurrent streams of one sweep each get one.
+void set_workspace_override(Workspace * w);
 UniqueMap unique_of(const int am[4]);
 const ClassKernels * find_kernels(const UniqueMap & u);
 int cart_index(int i, int j, int k, int ordering);

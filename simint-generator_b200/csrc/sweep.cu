@@ -113,6 +113,8 @@ __global__ void k_count_primq(const KernArgs a, unsigned long long * count)
 
 } // namespace
 
+#define SWEEP_SIDE 3                      // side streams besides the caller's
+
 struct simint_b200_basis
 {
     int nshell = 0;
@@ -126,6 +128,11 @@ struct simint_b200_basis
     std::map<std::array<long long, 3>, int> eager_done;
     long long graph_epoch = -1;            // settings_epoch() the graphs were built under
     cudaStream_t own_stream = nullptr;
+    // concurrent class streams of a full-layout sweep (fork/join around the
+    // classes); each side stream has its own scratch workspace
+    cudaStream_t side[SWEEP_SIDE] = {};
+    cudaEvent_t fork = nullptr, join[SWEEP_SIDE] = {};
+    Workspace side_ws[SWEEP_SIDE];
     int nlaunch = 0;
 };
 
@@ -444,6 +451,13 @@ extern "C" void simint_b200_basis_free(simint_b200_basis * b)
     for(auto & q : b->qcs)
         q.dev.release();
     b->dsums.release();
+    for(int i = 0; i < SWEEP_SIDE; i++)
+    {
+        if(b->side[i]) cudaStreamDestroy(b->side[i]);
+        if(b->join[i]) cudaEventDestroy(b->join[i]);
+        b->side_ws[i].dscratch.release();
+    }
+    if(b->fork) cudaEventDestroy(b->fork);
     delete b;
 }
 
@@ -539,6 +553,59 @@ static int issue_sweep(simint_b200_basis * b, int prec, double * dout, long long
 {
     int nl = 0;
     cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    if(!events && cap >= b->total_out)
+    {
+        // full layout: classes write disjoint output ranges, so they run on
+        // SWEEP_SIDE + 1 streams at once (small classes fill the GPU while
+        // large ones run).  Classes go to the least loaded stream, largest
+        // estimated cost first.
+        if(!b->fork)
+        {
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+            for(int i = 0; i < SWEEP_SIDE; i++)
+            {
+                cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+                cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+            }
+        }
+        std::vector<size_t> order(b->qcs.size());
+        std::iota(order.begin(), order.end(), 0);
+        // cost estimate from the task lists only (the same assignment on the
+        // eager run that sizes the workspaces and on the captured run)
+        auto cost = [&](size_t k) {
+            const QClass & q = b->qcs[k];
+            const int L = q.req[0] + q.req[1] + q.req[2] + q.req[3];
+            return (double)q.ntask * q.nout * (1.0 + L);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost(x) > cost(y); });
+        double load[SWEEP_SIDE + 1] = {};
+        cudaEventRecord(b->fork, stream);
+        for(int i = 0; i < SWEEP_SIDE; i++)
+            cudaStreamWaitEvent(b->side[i], b->fork, 0);
+        int rc = 0;
+        for(size_t k : order)
+        {
+            int s = 0;
+            for(int i = 1; i <= SWEEP_SIDE; i++)
+                if(load[i] < load[s]) s = i;
+            load[s] += cost(k);
+            set_workspace_override(s ? &b->side_ws[s - 1] : nullptr);
+            const int r = issue_class(b, k, prec, dout, cap, s ? b->side[s - 1] : stream);
+            set_workspace_override(nullptr);
+            if(r < 0)
+            {
+                rc = r;
+                break;
+            }
+            nl += r;
+        }
+        for(int i = 0; i < SWEEP_SIDE; i++)
+        {
+            cudaEventRecord(b->join[i], b->side[i]);
+            cudaStreamWaitEvent(stream, b->join[i], 0);
+        }
+        return rc < 0 ? rc : nl;
+    }
     for(size_t k = 0; k < b->qcs.size(); k++)
     {
         if(events)

@@ -28,16 +28,20 @@ PSI4, GAMESS = 0, 1
 FP64, MIXED = 0, 1
 
 _lib = None
+_libs = {}
 _dp = C.POINTER(C.c_double)
 
 EXPORTED = None  # filled from the headers by tests
 
 
 def load(path=LIBPATH):
-    """Load libsimint_b200.so (raises OSError when it is not built)."""
+    """Load libsimint_b200.so (raises OSError when it is not built); one
+    handle per path."""
     global _lib
-    if _lib is not None:
+    if path == LIBPATH and _lib is not None:
         return _lib
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise OSError("libsimint_b200.so not built: run simint-generator_b200/build.py")
     lib = C.CDLL(path)
@@ -60,7 +64,9 @@ def load(path=LIBPATH):
     lib.simint_b200_get_precision.restype = C.c_int
     lib.simint_b200_last_error.restype = C.c_char_p
     lib.simint_b200_launch_count.restype = C.c_longlong
-    _lib = lib
+    if path == LIBPATH:
+        _lib = lib
+    _libs[path] = lib
     return lib
 
 

@@ -45,8 +45,10 @@ def device_pairs(torch, lib, P):
     return torch.from_numpy(host).cuda()
 
 
-def build_case(lib, am, nbra, nket, nprim, seed, alpha=(0.05, 5e4), box=8.0):
-    """Shells and Schwarz-screened pair sets for an nbra x nket rectangle."""
+def build_case(lib, am, nbra, nket, nprim, seed, alpha=(0.05, 5e4), box=8.0,
+               screen=SIMINT_SCREEN_SCHWARZ):
+    """Shells and (by default Schwarz-screened) pair sets for an nbra x nket
+    rectangle."""
     rng = np.random.default_rng(seed)
     nA = max(1, int(round(np.sqrt(nbra))))
     nB = max(1, nbra // nA)
@@ -58,18 +60,20 @@ def build_case(lib, am, nbra, nket, nprim, seed, alpha=(0.05, 5e4), box=8.0):
     o = np.cumsum([0, nA, nB, nC, nD])
     bra = [(i, j) for i in range(o[0], o[1]) for j in range(o[1], o[2])]
     ket = [(i, j) for i in range(o[2], o[3]) for j in range(o[3], o[4])]
-    P = make_pairs(lib, S, bra, SIMINT_SCREEN_SCHWARZ)
-    Q = make_pairs(lib, S, ket, SIMINT_SCREEN_SCHWARZ)
+    P = make_pairs(lib, S, bra, screen)
+    Q = make_pairs(lib, S, ket, screen)
     return S, P, Q
 
 
 def run(am, prec="fp64", variant=None, nbra=32, nket=1024, nprim=(1, 4), reps=10, warmup=3,
-        tol=1e-14, gate=1e-6, deriv=0, seed=7, lib=None):
+        tol=1e-14, gate=1e-8, deriv=0, seed=7, lib=None, screen=SIMINT_SCREEN_SCHWARZ):
     import torch
     lib = lib or load()
     lib.simint_init()
     _bind(lib)
-    S, P, Q = build_case(lib, am, nbra, nket, nprim, seed)
+    S, P, Q = build_case(lib, am, nbra, nket, nprim, seed, screen=screen)
+    if not screen:
+        tol = 0.0
     dP, dQ = device_pairs(torch, lib, P), device_pairs(torch, lib, Q)
     nout = ncart(am[0]) * ncart(am[1]) * ncart(am[2]) * ncart(am[3]) * (12 if deriv else 1)
     nquart = P.nshell12_clip * Q.nshell12_clip
@@ -139,13 +143,15 @@ def main():
     ap.add_argument("--nprim", default="1,4")
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--gate", type=float, default=1e-6)
+    ap.add_argument("--gate", type=float, default=1e-8)
+    ap.add_argument("--no-screen", action="store_true", help="pairs without Schwarz values, tolerance 0")
     ap.add_argument("--seed", type=int, default=7)
     a = ap.parse_args()
     am = tuple(int(x) for x in a.am.split(","))
     nprim = tuple(int(x) for x in a.nprim.split(","))
     print(json.dumps(run(am, a.prec, a.variant, a.nbra, a.nket, nprim, a.reps, a.warmup,
-                         gate=a.gate, deriv=a.deriv, seed=a.seed)))
+                         gate=a.gate, deriv=a.deriv, seed=a.seed,
+                         screen=0 if a.no_screen else SIMINT_SCREEN_SCHWARZ)))
 
 
 if __name__ == "__main__":
