@@ -76,13 +76,9 @@ static inline int ci_flat(int i, int j, int k)
     return ci_lev_off(l) + ((l - i) * (l - i + 1)) / 2 + k;
 }
 
-static void upload_cart_info()
+// The table on the host (the same contents the device copy gets).
+static std::vector<CartInfo> cart_table_host()
 {
-    static int done_dev = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if(done_dev == dev)
-        return;
     std::vector<CartInfo> t(CI_NCART);
     for(int l = 0; l <= CI_MAXL; l++)
     {
@@ -113,6 +109,17 @@ static void upload_cart_info()
                 c.m2 = (short)(dir >= 0 ? ci_flat(q[0], q[1], q[2]) : -1);
             }
     }
+    return t;
+}
+
+static void upload_cart_info()
+{
+    static int done_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if(done_dev == dev)
+        return;
+    const std::vector<CartInfo> t = cart_table_host();
     cudaMemcpyToSymbol(c_cartinfo, t.data(), sizeof(CartInfo) * CI_NCART);
     done_dev = dev;
 }

@@ -83,6 +83,10 @@ struct C2Params
     int ordering;
     int res_size;                 // deriv 1: doubles of all target results per CTA
     int res_off[6];
+    const int2 * hrr_rows;        // HRR row tables (see c2_hrr_side)
+    int hrr_base[6][2];           // per target and side: first row
+    int hrr_loff[6][2][6];        // per target and side: row offsets of layers (relative)
+    int hrr_nl[6][2];             // per target and side: number of transfer layers
 };
 
 __device__ __forceinline__ int c2_lev_off(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
@@ -106,28 +110,31 @@ __device__ __forceinline__ int c2_index(const CartInfo * __restrict__ ci, int g,
 // One side of the HRR for every column at once, layer by layer in shared
 // memory.  in(g, col) gives the tops (functions on the top centre, levels
 // lo..lt); out(r, col, v) receives the (ta tb) block, r = pa * nc(tb) + pb.
-// Threads form a (row, column) grid so no element needs a division.
+// rows[loff[sl-1] .. loff[sl]) describe layer sl, one int2 per row:
+// x = source A | source B << 16 (function indices on layer 1, rows of the
+// previous layer after), y = direction | output row << 2 (last layer).
+// Threads form a (row, column) grid.
 template<int NT, typename IN, typename OUT>
-__device__ void c2_hrr_side(const CartInfo * __restrict__ ci, int right_step, int ta, int tb, int ncol,
-                            double X0, double X1, double X2, IN in, OUT out,
+__device__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * __restrict__ rows,
+                            const int * loff, double X0, double X1, double X2, IN in, OUT out,
                             double * __restrict__ LA, double * __restrict__ LB)
 {
-    const int lt = ta + tb;
-    const int lo = right_step ? ta : tb;
-    const int sl_max = right_step ? tb : ta;
-    const int nbb = c2_nc(tb);
     const int tid = threadIdx.x;
     const int TC = ncol < NT ? ncol : NT;
     const int TR = NT / TC;
     const int tc = tid % TC, tr = tid / TC;
+    const double Xs[3] = {right_step ? X0 : -X0, right_step ? X1 : -X1, right_step ? X2 : -X2};
     if(sl_max == 0)
     {
-        // nothing to transfer: the tops at level lt are the block
-        const int nr = c2_nc(ta) * nbb;
+        // nothing to transfer: row r of the block is top function rows[r].x
+        const int nr = loff[0];
         if(tr < TR)
             for(int r = tr; r < nr; r += TR)
+            {
+                const int g = __ldg(&rows[r].x);
                 for(int col = tc; col < ncol; col += TC)
-                    out(r, col, in(c2_lev_off(lt) + r, col));
+                    out(r, col, in(g, col));
+            }
         __syncthreads();
         return;
     }
@@ -135,44 +142,34 @@ __device__ void c2_hrr_side(const CartInfo * __restrict__ ci, int right_step, in
     const double * src = LB;
     for(int sl = 1; sl <= sl_max; sl++)
     {
-        // layer sl: (gt in levels lo..lt-sl) x (gs in level sl) x col
-        const int ngt = c2_lev_off(lt - sl + 1) - c2_lev_off(lo);
-        const int nsl = c2_nc(sl), nslm = c2_nc(sl - 1);
-        const int nrow = ngt * nsl;
+        const int r0 = loff[sl - 1], r1 = loff[sl];
         const bool last = sl == sl_max;
         if(tr < TR)
-            for(int r = tr; r < nrow; r += TR)
+            #pragma unroll 2
+            for(int r = r0 + tr; r < r1; r += TR)
             {
-                const int ps = r % nsl, itq = r / nsl;
-                const int it = c2_lev_off(lo) + itq;
-                const int is = c2_lev_off(sl) + ps;
-                const int x = ci[is].dir;
-                const int ism = ci[is].m1[x];
-                const int itp = ci[it].p1[x];
-                const int pm = ci[ism].pos;
-                double X = x == 0 ? X0 : (x == 1 ? X1 : X2);
-                if(!right_step)
-                    X = -X;
-                // on the last layer gt is at level lo: (pt, ps) -> (pa, pb)
-                const int orow = right_step ? itq * nbb + ps : ps * nbb + itq;
+                const int2 e = __ldg(&rows[r]);
+                const int a = e.x & 0xffff, b = (int)((unsigned)e.x >> 16);
+                const double X = Xs[e.y & 3];
+                const int orow = e.y >> 2;
                 if(sl == 1)
                 {
                     for(int col = tc; col < ncol; col += TC)
                     {
-                        const double v = fma(X, in(it, col), in(itp, col));
+                        const double v = fma(X, in(a, col), in(b, col));
                         if(last) out(orow, col, v);
-                        else dst[r * ncol + col] = v;
+                        else dst[(r - r0) * ncol + col] = v;
                     }
                 }
                 else
                 {
-                    const double * sa = src + ((it - c2_lev_off(lo)) * nslm + pm) * ncol;
-                    const double * sb = src + ((itp - c2_lev_off(lo)) * nslm + pm) * ncol;
+                    const double * sa = src + a * ncol;
+                    const double * sb = src + b * ncol;
                     for(int col = tc; col < ncol; col += TC)
                     {
                         const double v = fma(X, sa[col], sb[col]);
                         if(last) out(orow, col, v);
-                        else dst[r * ncol + col] = v;
+                        else dst[(r - r0) * ncol + col] = v;
                     }
                 }
             }
@@ -552,17 +549,20 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
             const int nket = c2_nc(tt[2]) * c2_nc(tt[3]);
             const int accb = p.acc_off[tg], accnf = p.acc_nf[tg];
             const int e0 = c2_lev_off(p.elo[tg]), f0 = c2_lev_off(p.flo[tg]), fk = c2_lev_off(klo);
-            c2_hrr_side<NT>(ci, p.brastep_j, tt[0], tt[1], ncol, c.AB[0], c.AB[1], c.AB[2],
+            c2_hrr_side<NT>(p.brastep_j, p.hrr_nl[ti][0], ncol, p.hrr_rows + p.hrr_base[ti][0],
+                            p.hrr_loff[ti][0], c.AB[0], c.AB[1], c.AB[2],
                             [&](int g, int col) { return acc[accb + (g - e0) * accnf + (fk + col - f0)]; },
                             [&](int r, int col, double v) { mid[r * ncol + col] = v; }, LA, LB);
             const int kl = c2_lev_off(klo);
             double * resd = res + p.res_off[ti];
             if(DERIV == 0)
-                c2_hrr_side<NT>(ci, p.ketstep_l, tt[2], tt[3], nbra, c.CD[0], c.CD[1], c.CD[2],
+                c2_hrr_side<NT>(p.ketstep_l, p.hrr_nl[ti][1], nbra, p.hrr_rows + p.hrr_base[ti][1],
+                                p.hrr_loff[ti][1], c.CD[0], c.CD[1], c.CD[2],
                                 [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
                                 [&](int r, int row, double v) { o[obra[row] + oket[r]] = v; }, LA, LB);
             else
-                c2_hrr_side<NT>(ci, p.ketstep_l, tt[2], tt[3], nbra, c.CD[0], c.CD[1], c.CD[2],
+                c2_hrr_side<NT>(p.ketstep_l, p.hrr_nl[ti][1], nbra, p.hrr_rows + p.hrr_base[ti][1],
+                                p.hrr_loff[ti][1], c.CD[0], c.CD[1], c.CD[2],
                                 [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
                                 [&](int r, int row, double v) { resd[row * nket + r] = v; }, LA, LB);
         }
@@ -657,8 +657,70 @@ struct C2Host
     int nthreads = 256;
     C2Params p;
     std::vector<C2Item> items;
-    std::map<int, C2Item *> dev_items;     // per device
+    std::vector<int2> hrr;                 // HRR row tables
+    std::map<int, char *> dev_tables;      // per device: items then HRR rows
 };
+
+// HRR row tables of every target and side (see c2_hrr_side).
+static bool c2_build_hrr(C2Params & p, std::vector<int2> & rows)
+{
+    const std::vector<CartInfo> ct = cart_table_host();
+    rows.clear();
+    for(int t = 0; t < p.ntarget; t++)
+        for(int side = 0; side < 2; side++)
+        {
+            const int * tt = p.tgt[t];
+            const int right = side == 0 ? p.brastep_j : p.ketstep_l;
+            const int ta = side == 0 ? tt[0] : tt[2], tb = side == 0 ? tt[1] : tt[3];
+            const int lt = ta + tb, lo = right ? ta : tb, slm = right ? tb : ta, nbb = nc2(tb);
+            if(slm > 5)
+                return false;
+            p.hrr_base[t][side] = (int)rows.size();
+            p.hrr_nl[t][side] = slm;
+            if(slm == 0)
+            {
+                const int nr = nc2(ta) * nbb;
+                for(int r = 0; r < nr; r++)
+                    rows.push_back(make_int2(lo_h(lt) + r, 0));
+                p.hrr_loff[t][side][0] = nr;
+                continue;
+            }
+            p.hrr_loff[t][side][0] = 0;
+            int cnt = 0;
+            for(int sl = 1; sl <= slm; sl++)
+            {
+                const int ngt = lo_h(lt - sl + 1) - lo_h(lo);
+                const int nsl = nc2(sl), nslm = nc2(sl - 1);
+                for(int r = 0; r < ngt * nsl; r++)
+                {
+                    const int ps = r % nsl, itq = r / nsl;
+                    const int it = lo_h(lo) + itq, is = lo_h(sl) + ps;
+                    const int x = ct[is].dir;
+                    const int ism = ct[is].m1[x];
+                    const int itp = ct[it].p1[x];
+                    const int pm = ct[ism].pos;
+                    int A, B;
+                    if(sl == 1)
+                    {
+                        A = it;
+                        B = itp;
+                    }
+                    else
+                    {
+                        A = (it - lo_h(lo)) * nslm + pm;
+                        B = (itp - lo_h(lo)) * nslm + pm;
+                    }
+                    const int orow = right ? itq * nbb + ps : ps * nbb + itq;
+                    if(A < 0 || A >= 65536 || B < 0 || B >= 65536)
+                        return false;
+                    rows.push_back(make_int2((int)((unsigned)A | ((unsigned)B << 16)), x | (orow << 2)));
+                    cnt++;
+                }
+                p.hrr_loff[t][side][sl] = cnt;
+            }
+        }
+    return true;
+}
 
 // Plan of one class for one variant (v = 0: the default, 256 threads, B = 4
 // halved until shared memory fits).
@@ -975,6 +1037,8 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
             ro += nc2(p.tgt[t][0]) * nc2(p.tgt[t][1]) * nc2(p.tgt[t][2]) * nc2(p.tgt[t][3]);
     }
     p.res_size = std::max(ro, 1);
+    if(!c2_build_hrr(p, h.hrr))
+        return false;
     return p.smem_doubles * 8 <= 200 * 1024 && nc2(am[0]) * nc2(am[1]) <= C2_MAXN
         && nc2(am[2]) * nc2(am[3]) <= C2_MAXN;
 }
@@ -1057,20 +1121,23 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
     C2Params p = h->p;
     {
         std::lock_guard<std::mutex> lk(g_c2_mutex);
-        auto it = h->dev_items.find(dev);
-        if(it == h->dev_items.end())
+        auto it = h->dev_tables.find(dev);
+        if(it == h->dev_tables.end())
         {
-            C2Item * d = nullptr;
-            if(cudaMalloc(&d, std::max<size_t>(1, h->items.size()) * sizeof(C2Item)) != cudaSuccess)
+            const size_t bi = h->items.size() * sizeof(C2Item), bh = h->hrr.size() * sizeof(int2);
+            char * d = nullptr;
+            if(cudaMalloc(&d, std::max<size_t>(16, bi + bh)) != cudaSuccess)
             {
                 cudaGetLastError();
                 set_error("out of device memory for cooperative-kernel tables");
                 return SIMINT_B200_ERR_CUDA;
             }
-            cudaMemcpy(d, h->items.data(), h->items.size() * sizeof(C2Item), cudaMemcpyHostToDevice);
-            it = h->dev_items.emplace(dev, d).first;
+            cudaMemcpy(d, h->items.data(), bi, cudaMemcpyHostToDevice);
+            cudaMemcpy(d + bi, h->hrr.data(), bh, cudaMemcpyHostToDevice);
+            it = h->dev_tables.emplace(dev, d).first;
         }
-        p.items = it->second;
+        p.items = (const C2Item *)it->second;
+        p.hrr_rows = (const int2 *)(it->second + h->items.size() * sizeof(C2Item));
     }
     p.ordering = ordering();
     a.swapB = a.swapK = a.pq = 0;
