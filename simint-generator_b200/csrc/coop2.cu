@@ -227,6 +227,12 @@ __device__ __forceinline__ void c2_boys(const double * __restrict__ tab, double 
     }
 }
 
+// Small non-negative integer n as a floating-point value without a
+// conversion instruction: the bits of 2^52 + n (resp. 2^23 + n) minus 2^52
+// (2^23), exact for n < 2^23.
+__device__ __forceinline__ void c2_small(int n, double & d) { d = __hiloint2double(0x43300000, n) - 4503599627370496.0; }
+__device__ __forceinline__ void c2_small(int n, float & f) { f = __int_as_float(0x4b000000 | n) - 8388608.0f; }
+
 // Coefficient combo of one prepared primitive quartet: X, Y, Z, 1/2s.
 __device__ __forceinline__ void c2_combo(const double * cf, int combo, double & X, double & Y, double & Z, double & O)
 {
@@ -250,7 +256,9 @@ __device__ __forceinline__ void c2_unit(const int4 q, const T * __restrict__ w1,
     const int o2 = q.y & 0xffff, o3 = (int)((unsigned)q.y >> 16);
     const int combo = (q.z >> 16) & 7;
     const bool has2 = (q.z >> 24) & 1, has3 = (q.z >> 25) & 1;
-    const T dA = (T)(q.w & 15), dB = (T)((q.w >> 4) & 15);
+    T dA, dB;
+    c2_small(q.w & 15, dA);
+    c2_small((q.w >> 4) & 15, dB);
     #pragma unroll
     for(int bb = 0; bb < NB; bb++)
     {
