@@ -136,8 +136,10 @@ int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first
- * cooperative kernel, 4 = generic kernel and 5 = register kernel run in FP64
- * even in mixed mode; 0 restores the default rule).
+ * cooperative kernel, 4 = generic kernel, 5 = register kernel run in FP64
+ * even in mixed mode and 100 + a cooperative code = that kernel in FP64 even
+ * in mixed mode (prec must be SIMINT_B200_PREC_MIXED); 0 restores the
+ * default rule).
  * Returns SIMINT_B200_ERR_ARG when the variant does not exist for the class.
  * Sweep graphs captured earlier are rebuilt on their next use. */
 int simint_b200_set_variant(const int am[4], int deriv, int prec, int variant);

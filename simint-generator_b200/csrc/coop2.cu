@@ -443,6 +443,10 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
             acc[k] = 0.0;
         const int ni = c.bi1 - c.bi0, nj = c.kj1 - c.kj0;
         const int ncand = ni * nj;
+        // k / nj as a multiply-high, exact while k * nj < 2^32; a division
+        // otherwise (contractions of thousands of primitive pairs)
+        const unsigned long long njinv = nj > 0 ? (1ull << 32) / (unsigned)nj + 1ull : 0ull;
+        const bool fastdiv = (long long)ncand * nj < (1LL << 32);
         for(int k0 = 0; k0 < ncand; k0 += NT)
         {
             // ordered compaction of the surviving primitive quartets k0..k0+NT
@@ -452,7 +456,8 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
             bool ok = false;
             if(k < ncand)
             {
-                const int i = c.bi0 + k / nj, j = c.kj0 + k % nj;
+                const int kq = fastdiv ? (int)(((unsigned long long)k * njinv) >> 32) : k / nj;
+                const int i = c.bi0 + kq, j = c.kj0 + (k - kq * nj);
                 const BraPrim bp = load_bra_prim(c, i);
                 ok = !(c.check && (bp.skip || !prim_survives(c, bp, j)));
             }
@@ -483,7 +488,8 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs 
                 if(tid < ng)
                 {
                     const int kk = surv[g0 + tid];
-                    const int i = c.bi0 + kk / nj, j = c.kj0 + kk % nj;
+                    const int kq = fastdiv ? (int)(((unsigned long long)kk * njinv) >> 32) : kk / nj;
+                    const int i = c.bi0 + kq, j = c.kj0 + (kk - kq * nj);
                     const BraPrim bp = load_bra_prim(c, i);
                     PrimSetup s;
                     prim_setup(c, bp, j, s);

@@ -476,6 +476,13 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
     a.boys = boys_table();
     const ClassKernels * k = deriv == 0 ? find_kernels(u) : nullptr;
     int v = variant_of(req, deriv, prec);
+    if(v >= 100)
+    {
+        // the FP64 form of a variant, chosen for a class in mixed mode
+        v -= 100;
+        prec = SIMINT_B200_PREC_FP64;
+        a.gate = 0.0;
+    }
     if(v == VAR_DEFAULT)
         // untuned default: the register kernel while its contracted tops fit
         // registers (above ~200 accumulators it spills), else cooperative
@@ -820,6 +827,10 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case 21: case 22: case 24:
         case 41: case 42: case 44:
             ok = coop2_supported(am, deriv, variant);
+            break;
+        case 121: case 122: case 124:
+        case 141: case 142: case 144:
+            ok = prec == SIMINT_B200_PREC_MIXED && coop2_supported(am, deriv, variant - 100);
             break;
         default:
             ok = false;

@@ -94,7 +94,8 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
 // Kernel variant per (requested class, deriv, precision), chosen by the
 // autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
 // 5 straight-line in FP64 even in mixed mode, 20+B / 40+B cooperative v2
-// with batch B and 256 / 128 threads.
+// with batch B and 256 / 128 threads; 100 + a cooperative code: that kernel
+// in FP64 even in mixed mode.
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5 };
 int variant_of(const int req[4], int deriv, int prec);
 void set_variant(const int req[4], int deriv, int prec, int v);

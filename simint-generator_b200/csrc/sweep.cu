@@ -648,7 +648,11 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
         }
         for(int v : {21, 22, 24, 41, 42, 44})
             if(coop2_supported(q.req, 0, v))
+            {
                 cand.push_back(v);
+                if(prec == SIMINT_B200_PREC_MIXED)
+                    cand.push_back(v + 100);      // the same kernel without the FP32 path
+            }
         if(cand.empty())
             continue;
         int best = cand[0];

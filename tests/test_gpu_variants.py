@@ -71,3 +71,26 @@ def test_every_variant_matches_oracle(libs, am, deriv):
         lib.simint_free_multi_shellpair(C.byref(P))
         lib.simint_free_multi_shellpair(C.byref(Q))
     assert sb.VAR_GENERIC in ran and len(ran) >= 2, ran
+
+
+@pytest.mark.parametrize("am", [(2, 2, 2, 2), (3, 2, 2, 1)], ids=lambda a: "".join("spdfg"[x] for x in a))
+def test_fp64_forms_under_mixed_mode(libs, am):
+    """Codes 100 + v run the cooperative kernel without its FP32 path in
+    mixed mode: FP64 parity holds whatever the gate."""
+    lib, orc = libs
+    S, bra, ket, rr, ref = _case(lib, orc, am, 0, 99 + sum(am))
+    P = sb.make_pairs(lib, S, bra, sb.SIMINT_SCREEN_SCHWARZ)
+    Q = sb.make_pairs(lib, S, ket, sb.SIMINT_SCREEN_SCHWARZ)
+    try:
+        lib.simint_b200_set_precision(sb.MIXED, 1e30)
+        for v in (124, 142):
+            assert sb.set_variant(am, v, 0, sb.MIXED, lib) == 0
+            r, out = sb.compute_eri(P, Q, 0.0, 0, lib)
+            bad, dmax = parity_bad(out, ref)
+            assert len(bad) == 0, (v, dmax)
+        assert sb.set_variant(am, 124, 0, sb.FP64, lib) != 0       # mixed mode only
+    finally:
+        lib.simint_b200_set_precision(sb.FP64, 0.0)
+        sb.set_variant(am, sb.VAR_DEFAULT, 0, sb.MIXED, lib)
+        lib.simint_free_multi_shellpair(C.byref(P))
+        lib.simint_free_multi_shellpair(C.byref(Q))
