@@ -121,6 +121,17 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+METRIC = "primitive quartets/s (cfg2 l<=3 screened sweep sample, screen_tol 1e-14)"
+
+
+def workload_config(args, world=1):
+    """The workload description both arms print."""
+    return {"workload": "cfg2 sweep sample: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, "
+                        "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14; every %d-th bra "
+                        "row of every class per rank (rank r: rows r mod %d)" % (args.stride, args.stride),
+            "parallelism": "dp%d (disjoint row shards, no data-path collective)" % world}
+
+
 def workload_shells(lib):
     from simint_b200.capi import ShellSet
     from simint_b200.workloads import config_shells
@@ -210,13 +221,12 @@ def run_reference(args):
     rate = statistics.median(v[0] for v in vals)
     t = statistics.median(v[1] for v in vals)
     out = {
-        "impl": "reference", "metric": "primitive quartets/s (cfg2 l<=3 sweep sample, screen_tol 1e-14)",
+        "impl": "reference", "metric": METRIC,
         "value": rate, "unit": "primitive quartets/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 shells)",
-        "config": {"workload": "cfg2: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, 120 atoms, "
-                               "Schwarz 1e-14; simint_compute_eri rows (1 bra pair x screened kets)",
-                   "sample_rows": vals[-1][3], "l2": "n/a (CPU)"},
+        "config": dict(workload_config(args), sample_rows=vals[-1][3], l2="n/a (CPU)",
+                       timed="simint_compute_eri-shaped rows (1 bra pair x screened kets) of the sample"),
         "cpu_baseline": {"value": rate, "unit": "primitive quartets/s", "cores": threads,
                          "kind": "port",
                          "sample": "%d simint_compute_eri-shaped rows of the cfg2 sweep sample, %.3g primitive quartets"
@@ -393,18 +403,17 @@ def run_b200(args):
     if rank == 0:
         launches = nlmx // 2 * args.steps      # ERI kernels (checksum kernels excluded)
         res = {
-            "metric": "primitive quartets/s, mixed-precision batched sweep (cfg2 l<=3, screen 1e-14)",
+            "metric": METRIC,
             "value": value, "unit": "primitive quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the error-estimate gate)",
             "data": "synthetic (seeded cfg2 shells, PCG64 seed 2024)",
-            "config": {"workload": "cfg2 sweep sample: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, "
-                                   "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14; every %d-th bra "
-                                   "row of every class per rank (rank r: rows r mod %d)" % (args.stride, args.stride),
+            "config": dict(workload_config(args, world), **{
+                       "path": "mixed-precision batched sweep (value); FP64 sweep in fp64",
                        "quartets_per_step": int(sum(c["nquart"] for c in classes)),
                        "primq_per_step": int(total_npq), "full_sweep_quartets": int(nfull),
                        "gate": gate, "l2": "256 MB flush before every timed step",
-                       "parallelism": "dp%d (disjoint row shards, no data-path collective)" % world, "setup_s": round(setup_s, 1), "autotune_s": round(tune_s, 1)},
+                       "setup_s": round(setup_s, 1), "autotune_s": round(tune_s, 1)}),
             "fp64": {"value": value64, "ms_per_step": ms64},
             "mixed_vs_fp64": {"max_abs_err": max((e[0] for e in errs.values()), default=None),
                               "max_rel_err": max((e[1] for e in errs.values()), default=None),

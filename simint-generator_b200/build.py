@@ -92,7 +92,7 @@ def build(max_am=4, limit=DEFAULT_LIMIT, jobs=None, verbose=False, only=None):
             if dt > 0:
                 logs.append((src, dt, err))
     if logs or not os.path.exists(LIB) or not _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))

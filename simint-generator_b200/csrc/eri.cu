@@ -29,6 +29,7 @@
 #include "simint_b200.h"
 #include "kernels.h"
 #include "runtime.h"
+#include "hostpool.h"
 #include "gen/boys_grid.inc"
 
 namespace sb200 {
@@ -320,27 +321,31 @@ size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L
         return total;
     double * rec = (double *)(dst + L.off_rec);
     const bool has_screen = P->screen != nullptr;
-    for(int s = 0; s < npad; s++)
-    {
-        double * r = rec + (size_t)s * SB_REC;
-        r[0] = P->alpha[s]; r[1] = P->prefac[s];
-        r[2] = P->x[s]; r[3] = P->y[s]; r[4] = P->z[s];
-        r[5] = P->PA_x[s]; r[6] = P->PA_y[s]; r[7] = P->PA_z[s];
-        r[8] = P->PB_x[s]; r[9] = P->PB_y[s]; r[10] = P->PB_z[s];
-        r[11] = P->alpha2 ? P->alpha2[s] : 0.0;
-        r[12] = P->beta2 ? P->beta2[s] : 0.0;
-        const double sc = has_screen ? P->screen[s] : 0.0;
-        r[13] = sc;
-        r[15] = has_screen ? std::sqrt(std::max(sc, 0.0)) : INFINITY;
-    }
-    for(int g = 0; g < npad; g += 8)
-    {
-        double m = 0.0;
-        for(int s = g; s < std::min(g + 8, npad); s++)
-            m = std::max(m, rec[(size_t)s * SB_REC + 13]);
-        for(int s = g; s < std::min(g + 8, npad); s++)
-            rec[(size_t)s * SB_REC + 14] = m;
-    }
+    // records in groups of 8 slots (the vector-screening groups), spread
+    // over the host pool for large sets
+    parallel_for((size_t)(npad + 7) / 8, 2048, [&](size_t g0, size_t g1) {
+        for(int g = (int)g0 * 8; g < std::min((int)g1 * 8, npad); g += 8)
+        {
+            double m = 0.0;
+            const int ge = std::min(g + 8, npad);
+            for(int s = g; s < ge; s++)
+            {
+                double * r = rec + (size_t)s * SB_REC;
+                r[0] = P->alpha[s]; r[1] = P->prefac[s];
+                r[2] = P->x[s]; r[3] = P->y[s]; r[4] = P->z[s];
+                r[5] = P->PA_x[s]; r[6] = P->PA_y[s]; r[7] = P->PA_z[s];
+                r[8] = P->PB_x[s]; r[9] = P->PB_y[s]; r[10] = P->PB_z[s];
+                r[11] = P->alpha2 ? P->alpha2[s] : 0.0;
+                r[12] = P->beta2 ? P->beta2[s] : 0.0;
+                const double sc = has_screen ? P->screen[s] : 0.0;
+                r[13] = sc;
+                r[15] = has_screen ? std::sqrt(std::max(sc, 0.0)) : INFINITY;
+                m = std::max(m, sc);
+            }
+            for(int s = g; s < ge; s++)
+                rec[(size_t)s * SB_REC + 14] = m;
+        }
+    });
     memcpy(dst + L.off_start, start.data(), P->nshell12 * sizeof(int));
     memcpy(dst + L.off_nprim, P->nprim12, P->nshell12 * sizeof(int));
     double * ab = (double *)(dst + L.off_AB);
@@ -600,7 +605,11 @@ extern "C" int simint_compute_eri_deriv(int deriv,
                              precision(), gate(), (double *)w.dout.ptr, w.stream);
     if(r < 0)
         return r;
-    cudaMemcpyAsync(integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost, w.stream);
+    // results through the pinned staging buffer (full-speed DMA), then into
+    // the caller's memory on all host cores
+    const bool staged = outbytes >= (1u << 20) && w.hout.reserve(outbytes);
+    cudaMemcpyAsync(staged ? w.hout.ptr : (void *)integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost,
+                    w.stream);
     cudaError_t e = cudaStreamSynchronize(w.stream);
     if(e == cudaSuccess)
         e = cudaGetLastError();
@@ -609,6 +618,8 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
         return SIMINT_B200_ERR_CUDA;
     }
+    if(staged)
+        parallel_copy(integrals, w.hout.ptr, outbytes);
     return (int)nquart;
 }
 
