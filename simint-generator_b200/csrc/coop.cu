@@ -786,6 +786,7 @@ extern "C" int simint_b200_compute_eri_noalloc(int deriv,
     a.kord = d.kord;
     a.ntask = ntask;
     a.nQ = Q->nshell12_clip;
+    a.nQc = a.nQ;
     a.check = (screen_tol > 0.0) && P->screen && Q->screen;
     a.tol2 = tol2;
     a.out = dev_integrals;

@@ -305,32 +305,20 @@ void pair_starts(const simint_multi_shellpair * P, std::vector<int> & start, int
 }
 
 // Pack one pair set into host staging memory: records, starts, counts, AB.
-size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L)
+// Records of padded slots [g0, g1) (multiples of 8, the vector-screening
+// groups) into rec (slot 0 of rec = slot g0), on the host pool.
+void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, double * rec)
 {
-    std::vector<int> start;
-    int npad = 0;
-    pair_starts(P, start, npad);
-    L.npad = npad;
-    L.npair = P->nshell12;
-    L.off_rec = 0;
-    L.off_start = (size_t)npad * SB_REC * sizeof(double);
-    L.off_nprim = L.off_start + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
-    L.off_AB = L.off_nprim + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
-    const size_t total = L.off_AB + 3 * (size_t)P->nshell12 * sizeof(double);
-    if(!dst)
-        return total;
-    double * rec = (double *)(dst + L.off_rec);
     const bool has_screen = P->screen != nullptr;
-    // records in groups of 8 slots (the vector-screening groups), spread
-    // over the host pool for large sets
-    parallel_for((size_t)(npad + 7) / 8, 2048, [&](size_t g0, size_t g1) {
-        for(int g = (int)g0 * 8; g < std::min((int)g1 * 8, npad); g += 8)
+    g1 = std::min(g1, npad);
+    parallel_for((size_t)(g1 - g0 + 7) / 8, 2048, [&](size_t b0, size_t b1) {
+        for(int g = g0 + (int)b0 * 8; g < std::min(g0 + (int)b1 * 8, g1); g += 8)
         {
             double m = 0.0;
-            const int ge = std::min(g + 8, npad);
+            const int ge = std::min(g + 8, g1);
             for(int s = g; s < ge; s++)
             {
-                double * r = rec + (size_t)s * SB_REC;
+                double * r = rec + (size_t)(s - g0) * SB_REC;
                 r[0] = P->alpha[s]; r[1] = P->prefac[s];
                 r[2] = P->x[s]; r[3] = P->y[s]; r[4] = P->z[s];
                 r[5] = P->PA_x[s]; r[6] = P->PA_y[s]; r[7] = P->PA_z[s];
@@ -343,9 +331,32 @@ size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L
                 m = std::max(m, sc);
             }
             for(int s = g; s < ge; s++)
-                rec[(size_t)s * SB_REC + 14] = m;
+                rec[(size_t)(s - g0) * SB_REC + 14] = m;
         }
     });
+}
+
+// Layout of the packed pair set: records, then starts, counts and AB at
+// 256-byte aligned offsets; optionally the padded start of every pair.
+static size_t pack_layout(const simint_multi_shellpair * P, PackedLayout & L, std::vector<int> * start_out)
+{
+    std::vector<int> start;
+    int npad = 0;
+    pair_starts(P, start, npad);
+    L.npad = npad;
+    L.npair = P->nshell12;
+    L.off_rec = 0;
+    L.off_start = (size_t)npad * SB_REC * sizeof(double);
+    L.off_nprim = L.off_start + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    L.off_AB = L.off_nprim + ((P->nshell12 * sizeof(int) + 255) & ~(size_t)255);
+    if(start_out)
+        start_out->swap(start);
+    return L.off_AB + 3 * (size_t)P->nshell12 * sizeof(double);
+}
+
+static void pack_meta(const simint_multi_shellpair * P, const PackedLayout & L, const std::vector<int> & start,
+                      char * dst)
+{
     memcpy(dst + L.off_start, start.data(), P->nshell12 * sizeof(int));
     memcpy(dst + L.off_nprim, P->nprim12, P->nshell12 * sizeof(int));
     double * ab = (double *)(dst + L.off_AB);
@@ -355,6 +366,17 @@ size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L
         ab[3 * p + 1] = P->AB_y[p];
         ab[3 * p + 2] = P->AB_z[p];
     }
+}
+
+// Pack one pair set into host staging memory: records, starts, counts, AB.
+size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L)
+{
+    std::vector<int> start;
+    const size_t total = pack_layout(P, L, &start);
+    if(!dst)
+        return total;
+    pack_records(P, L.npad, 0, L.npad, (double *)(dst + L.off_rec));
+    pack_meta(P, L, start, dst);
     return total;
 }
 
@@ -525,7 +547,7 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
 int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
                      const simint_multi_shellpair * Q, const PairSetDev & dQ,
                      const int * dkord, double screen_tol, int deriv, int prec, double gatev,
-                     double * dout, cudaStream_t stream)
+                     double * dout, cudaStream_t stream, int nqc)
 {
     const int req[4] = {P->am1, P->am2, Q->am1, Q->am2};
     const int nc = ncart(req[0]) * ncart(req[1]) * ncart(req[2]) * ncart(req[3]);
@@ -534,8 +556,9 @@ int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
     a.P = dP;
     a.Q = dQ;
     a.kord = dkord;
-    a.ntask = (long long)P->nshell12_clip * Q->nshell12_clip;
     a.nQ = Q->nshell12_clip;
+    a.nQc = nqc < 0 ? a.nQ : nqc;
+    a.ntask = (long long)P->nshell12_clip * a.nQc;
     a.check = (screen_tol > 0.0) && P->screen && Q->screen;
     a.tol2 = screen_tol * screen_tol;
     a.gate = (prec == SIMINT_B200_PREC_MIXED) ? gatev : 0.0;
@@ -545,6 +568,136 @@ int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
 }
 
 } // namespace sb200
+
+// Large calls: the ket pairs go through the device in chunks (multiples of
+// 16 pairs, so chunk records are whole padded groups) so host packing of
+// chunk k+1 and the copy of chunk k-1's results into the caller's memory run
+// while the GPU uploads, computes and downloads chunk k.  Results are the
+// same as the one-shot path (each chunk's kets in primitive-count order).
+static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, const simint_multi_shellpair * Q,
+                                 double screen_tol, double * integrals, int nc)
+{
+    Workspace & w = workspace();
+    const int nP = P->nshell12_clip, nQ = Q->nshell12_clip;
+    const size_t outbytes = (size_t)nP * nQ * nc * sizeof(double);
+    // few chunks: each launch must still fill the GPU
+    const int nch = (int)std::min<size_t>(4, std::max<size_t>(2, outbytes / ((size_t)32 << 20)));
+    const int cq = std::max(16, ((nQ + nch - 1) / nch + 15) & ~15);
+    PackedLayout LP, LQ;
+    std::vector<int> qstart;
+    const size_t szP = (pack_pairs(P, nullptr, LP) + 255) & ~(size_t)255;
+    const size_t szQ = (pack_layout(Q, LQ, &qstart) + 255) & ~(size_t)255;
+    const size_t szK = ((size_t)nQ * sizeof(int) + 255) & ~(size_t)255;
+    // staging: P | Q meta (records area unused) | two chunk slots (records + kord)
+    size_t maxrec = 0;
+    for(int c0 = 0; c0 < nQ; c0 += cq)
+    {
+        const int c1 = std::min(nQ, c0 + cq);
+        const int g0 = qstart[c0], g1 = c1 >= nQ ? LQ.npad : qstart[c1];
+        maxrec = std::max(maxrec, (size_t)(g1 - g0) * SB_REC * sizeof(double));
+    }
+    const size_t slot = ((maxrec + (size_t)cq * sizeof(int)) + 255) & ~(size_t)255;
+    if(!w.hstage.reserve(szP + szQ + 2 * slot) || !w.dpair.reserve(szP + szQ + szK) || !w.dout.reserve(outbytes)
+       || !w.hout.reserve(outbytes))
+    {
+        set_error("out of memory for a pipelined call");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    char * h = (char *)w.hstage.ptr;
+    char * d = (char *)w.dpair.ptr;
+    pack_pairs(P, h, LP);
+    pack_meta(Q, LQ, qstart, h + szP);
+    // P, and Q's starts/counts/AB (everything after the records)
+    cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream);
+    cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start, cudaMemcpyHostToDevice,
+                    w.stream);
+    const PairSetDev dP = device_view(d, LP, P->screen_max);
+    const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
+    int * dkord = (int *)(d + szP + szQ);
+    if(!w.dstream && cudaStreamCreateWithFlags(&w.dstream, cudaStreamNonBlocking) != cudaSuccess)
+    {
+        set_error("cudaStreamCreate failed");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    static thread_local std::vector<cudaEvent_t> ev;
+    const int nchunk = (nQ + cq - 1) / cq;
+    while((int)ev.size() < 2 * nchunk + 2)
+    {
+        cudaEvent_t e;
+        if(cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        {
+            set_error("cudaEventCreate failed");
+            return SIMINT_B200_ERR_CUDA;
+        }
+        ev.push_back(e);
+    }
+    const size_t rowbytes = (size_t)nQ * nc * sizeof(double);
+    auto copy_out = [&](int k) {
+        const int c0 = k * cq, c1 = std::min(nQ, c0 + cq);
+        const size_t off = (size_t)c0 * nc * sizeof(double), len = (size_t)(c1 - c0) * nc * sizeof(double);
+        if(nP == 1)
+            parallel_copy((char *)integrals + off, (char *)w.hout.ptr + off, len);
+        else
+            parallel_for((size_t)nP, 1, [&](size_t r0, size_t r1) {
+                for(size_t r = r0; r < r1; r++)
+                    memcpy((char *)integrals + r * rowbytes + off, (char *)w.hout.ptr + r * rowbytes + off, len);
+            });
+    };
+    int rc = 0;
+    for(int k = 0; k < nchunk && rc == 0; k++)
+    {
+        const int c0 = k * cq, c1 = std::min(nQ, c0 + cq);
+        const int g0 = qstart[c0], g1 = c1 >= nQ ? LQ.npad : qstart[c1];
+        char * hs = h + szP + szQ + (size_t)(k & 1) * slot;
+        if(k >= 2)
+            cudaEventSynchronize(ev[k & 1]);           // staging slot of chunk k-2 uploaded
+        pack_records(Q, LQ.npad, g0, g1, (double *)hs);
+        const size_t recbytes = (size_t)(g1 - g0) * SB_REC * sizeof(double);
+        int * kk = (int *)(hs + recbytes);
+        for(int q = c0; q < c1; q++) kk[q - c0] = q;
+        std::stable_sort(kk, kk + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+        cudaMemcpyAsync(d + szP + (size_t)g0 * SB_REC * sizeof(double), hs, recbytes, cudaMemcpyHostToDevice,
+                        w.stream);
+        cudaMemcpyAsync(dkord + c0, kk, (size_t)(c1 - c0) * sizeof(int), cudaMemcpyHostToDevice, w.stream);
+        cudaEventRecord(ev[k & 1], w.stream);
+        rc = launch_rectangle(P, dP, Q, dQ, dkord + c0, screen_tol, deriv, precision(), gate(),
+                              (double *)w.dout.ptr, w.stream, c1 - c0);
+        if(rc < 0)
+            break;
+        rc = 0;
+        // the download of chunk k overlaps the upload and kernel of chunk k+1
+        const size_t off = (size_t)c0 * nc * sizeof(double), len = (size_t)(c1 - c0) * nc * sizeof(double);
+        cudaEventRecord(ev[2 + nchunk + k], w.stream);
+        cudaStreamWaitEvent(w.dstream, ev[2 + nchunk + k], 0);
+        if(nP == 1)
+            cudaMemcpyAsync((char *)w.hout.ptr + off, (char *)w.dout.ptr + off, len, cudaMemcpyDeviceToHost,
+                            w.dstream);
+        else
+            cudaMemcpy2DAsync((char *)w.hout.ptr + off, rowbytes, (char *)w.dout.ptr + off, rowbytes, len, nP,
+                              cudaMemcpyDeviceToHost, w.dstream);
+        cudaEventRecord(ev[2 + k], w.dstream);
+        if(k >= 1)
+        {
+            cudaEventSynchronize(ev[2 + k - 1]);
+            copy_out(k - 1);
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(w.stream);
+    const cudaError_t e2 = cudaStreamSynchronize(w.dstream);
+    if(e == cudaSuccess)
+        e = e2;
+    if(e == cudaSuccess)
+        e = cudaGetLastError();
+    if(rc < 0)
+        return rc;
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    copy_out(nchunk - 1);
+    return nP * nQ;
+}
 
 extern "C" int simint_compute_eri_deriv(int deriv,
                                         struct simint_multi_shellpair const * P,
@@ -573,6 +726,11 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     const long long nquart = (long long)P->nshell12_clip * Q->nshell12_clip;
     if(nquart == 0)
         return 0;
+    {
+        const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);
+        if((size_t)nquart * nc * sizeof(double) >= ((size_t)16 << 20) && Q->nshell12_clip >= 64)
+            return compute_eri_pipelined(deriv, P, Q, screen_tol, integrals, nc);
+    }
     PackedLayout LP, LQ;
     const size_t szP = (pack_pairs(P, nullptr, LP) + 255) & ~(size_t)255;
     const size_t szQ = (pack_pairs(Q, nullptr, LQ) + 255) & ~(size_t)255;

@@ -35,7 +35,8 @@ struct KernArgs
     const int2 * tasks;       // list mode: (bra pair, ket pair)
     const long long * outoff; // list mode: output offset of each task (doubles)
     long long ntask;
-    int nQ;                   // rectangle mode: number of ket pairs
+    int nQ;                   // rectangle mode: number of ket pairs (output stride)
+    int nQc;                  // rectangle mode: ket pairs of this launch (kord entries)
     int swapB, swapK, pq;     // role swaps (see emit.unique_class)
     int check;                // screening on
     double tol2;              // squared tolerance
@@ -322,7 +323,8 @@ __device__ __forceinline__ void make_ctx(const KernArgs & a, int iP, int iQ, Qua
 }
 
 // Map a thread to a shell quartet.  MODE 0: the P x Q rectangle of
-// simint_compute_eri, kets visited in the order kord (sorted by primitive
+// simint_compute_eri (or the P x (nQc kets) part of it one launch of a
+// chunked call covers), kets visited in the order kord (sorted by primitive
 // count so a warp's loops have equal trip counts); output at
 // (iP*nQ + iQ)*nout.  MODE 1: an explicit task list.
 template<int MODE>
@@ -333,8 +335,8 @@ __device__ __forceinline__ bool task_of(const KernArgs & a, long long t, int & i
         return false;
     if(MODE == 0)
     {
-        iP = (int)(t / a.nQ);
-        iQ = a.kord[t - (long long)iP * a.nQ];
+        iP = (int)(t / a.nQc);
+        iQ = a.kord[t - (long long)iP * a.nQc];
         off = ((long long)iP * a.nQ + iQ) * a.nout;
     }
     else if(MODE == 1)

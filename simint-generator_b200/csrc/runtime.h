@@ -37,6 +37,7 @@ struct HostBuf
 struct Workspace
 {
     cudaStream_t stream = nullptr;
+    cudaStream_t dstream = nullptr;       // downloads of pipelined calls
     DevBuf dpair, dout, dkord, dscratch;
     HostBuf hstage, hout;
     ~Workspace();
@@ -69,10 +70,13 @@ size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L
 PairSetDev device_view(const char * base, const PackedLayout & L, double screen_max);
 const unsigned short * oidx_table(const int req[4], const UniqueMap & u, int ord);
 
+// The P x Q rectangle (nqc < 0), or its part P x (kets dkord[0..nqc)) with
+// the rectangle's output layout.
 int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
                      const simint_multi_shellpair * Q, const PairSetDev & dQ,
                      const int * dkord, double screen_tol, int deriv, int prec, double gatev,
-                     double * dout, cudaStream_t stream);
+                     double * dout, cudaStream_t stream, int nqc = -1);
+void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, double * rec);
 
 int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
                  cudaStream_t stream);
