@@ -137,7 +137,9 @@ int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first
  * cooperative kernel, 4 = generic kernel, 5 = register kernel run in FP64
- * even in mixed mode and 100 + a cooperative code = that kernel in FP64 even
+ * even in mixed mode, 6 = register kernel with one warp per shell quartet,
+ * 7 = the same in FP64 even in mixed mode, and 100 + a cooperative code =
+ * that kernel in FP64 even
  * in mixed mode (prec must be SIMINT_B200_PREC_MIXED); 0 restores the
  * default rule).
  * Returns SIMINT_B200_ERR_ARG when the variant does not exist for the class.

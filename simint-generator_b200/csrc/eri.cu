@@ -529,6 +529,21 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         count_launch(1);
         return 0;
     }
+    if((v == VAR_WARP || v == VAR_WARP64) && k && k->fnw[mode][0])
+    {
+        a.oidx = oidx_table(req, u, ordering());
+        if(!a.oidx)
+        {
+            set_error("cannot allocate output index table");
+            return SIMINT_B200_ERR_CUDA;
+        }
+        const int threads = 128;           // 4 shell quartets per block
+        const long long blocks = (a.ntask + 3) / 4;
+        KernFn fn = k->fnw[mode][(prec == SIMINT_B200_PREC_MIXED && v == VAR_WARP) ? 1 : 0];
+        fn<<<(unsigned)blocks, threads, 0, stream>>>(a);
+        count_launch(1);
+        return 0;
+    }
     if(coop2_is_variant(v) && coop2_supported(req, deriv, v))
         return launch_coop2(a, req, deriv, mode, prec, stream, v);
     if(v == VAR_COOP1 && coop_supported(req, deriv))
@@ -927,6 +942,12 @@ bool has_straight(const int req[4])
     return find_kernels(unique_of(req)) != nullptr;
 }
 
+bool has_warp(const int req[4], int mode)
+{
+    const ClassKernels * k = find_kernels(unique_of(req));
+    return k && k->fnw[mode][0];
+}
+
 // Tuning cache: a small JSON object {"a,b,c,d,deriv,prec": variant, ...}
 // at $SIMINT_B200_TUNE_FILE, read at simint_init and written by the
 // autotuner.
@@ -989,6 +1010,10 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case VAR_STRAIGHT:
         case VAR_STRAIGHT64:
             ok = deriv == 0 && has_straight(am);
+            break;
+        case VAR_WARP:
+        case VAR_WARP64:
+            ok = deriv == 0 && has_warp(am, 0) && has_warp(am, 2);
             break;
         case VAR_COOP1:
             ok = coop_supported(am, deriv);

@@ -13,6 +13,7 @@ struct ClassKernels
     int vrr_flops;       // per primitive quartet (minimal plan)
     int hrr_flops;       // per shell quartet
     KernFn fn[3][2];     // [mode: 0 rectangle, 1 task list, 2 screened sweep][prec: 0 FP64, 1 mixed]
+    KernFn fnw[3][2];    // warp per shell quartet (modes 0 and 2)
 };
 
 struct KernelTable

@@ -97,10 +97,12 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
 
 // Kernel variant per (requested class, deriv, precision), chosen by the
 // autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
-// 5 straight-line in FP64 even in mixed mode, 20+B / 40+B cooperative v2
+// 5 straight-line in FP64 even in mixed mode, 6 (7) straight-line with a
+// warp per shell quartet (in FP64 even in mixed mode), 20+B / 40+B cooperative v2
 // with batch B and 256 / 128 threads; 100 + a cooperative code: that kernel
 // in FP64 even in mixed mode.
-enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5 };
+enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5,
+       VAR_WARP = 6, VAR_WARP64 = 7 };
 int variant_of(const int req[4], int deriv, int prec);
 void set_variant(const int req[4], int deriv, int prec, int v);
 // Incremented whenever a setting that captured sweep graphs bake in changes
@@ -108,6 +110,7 @@ void set_variant(const int req[4], int deriv, int prec, int v);
 long long settings_epoch();
 void bump_settings_epoch();
 bool has_straight(const int req[4]);
+bool has_warp(const int req[4], int mode);
 void save_tune_file();
 int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_t stream);
 int pair_diag_max(const PairSetDev & dP, int am1, int am2, int n, double * dmax, cudaStream_t stream);

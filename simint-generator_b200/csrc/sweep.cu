@@ -646,6 +646,12 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
             if(prec == SIMINT_B200_PREC_MIXED)
                 cand.push_back(VAR_STRAIGHT64);
         }
+        if(has_warp(q.req, 2))
+        {
+            cand.push_back(VAR_WARP);
+            if(prec == SIMINT_B200_PREC_MIXED)
+                cand.push_back(VAR_WARP64);
+        }
         for(int v : {21, 22, 24, 41, 42, 44})
             if(coop2_supported(q.req, 0, v))
             {

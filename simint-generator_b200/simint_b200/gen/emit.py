@@ -71,10 +71,14 @@ def _fmt_int(n):
     return "%d.0" % n
 
 
-def emit_class(am, prec="f64"):
+def emit_class(am, prec="f64", warp=False):
     """Return CUDA source text for the device function of unique class am.
 
-    prec: "f64" or "mixed"."""
+    prec: "f64" or "mixed".  warp: the function runs on a whole warp for one
+    shell quartet -- lanes take the (bra, ket) primitive pairs k = lane,
+    lane + 32, ... (no divergence between quartets of different contraction
+    depth), the top accumulators are summed over the warp by a butterfly,
+    and lane 0 does the HRR and the stores."""
     p = class_plan(*am)
     assert p.deriv == 0
     name = cname(am)
@@ -88,18 +92,32 @@ def emit_class(am, prec="f64"):
     w = o.append
     w("// ---- class (%s) : L=%d, %d top quartets, %d VRR elements, %d HRR steps"
       % (name, L, ntop, len(vrr), sum(1 for _, r in hrr if r is not None)))
-    fn = "ostei_%s_%s" % (name, prec)
+    fn = "ostei_%s_%s%s" % (name, prec, "_w" if warp else "")
     w("template<bool MIXED_GATE>")
     w("__device__ __forceinline__ void %s(const QuartetCtx& c, double* __restrict__ out)" % fn)
     w("{")
     for k in range(ntop):
         w("    double acc%d = 0.0;" % k)
-    w("    for(int i = c.bi0; i < c.bi1; ++i)")
-    w("    {")
-    w("        const BraPrim bp = load_bra_prim(c, i);")
-    w("        if(c.check && bp.skip) continue;")
-    w("        for(int j = c.kj0; j < c.kj1; ++j)")
-    w("        {")
+    if warp:
+        w("    const int lane = threadIdx.x & 31;")
+        w("    const int nj = c.kj1 - c.kj0, ncand = (c.bi1 - c.bi0) * nj;")
+        w("    // k / nj as a multiply-high, exact while k * nj < 2^32")
+        w("    const unsigned long long njinv = (1ull << 32) / (unsigned)max(nj, 1) + 1ull;")
+        w("    const bool fastdiv = (long long)ncand * nj < (1LL << 32);")
+        w("    for(int k = lane; k < ncand; k += 32)")
+        w("    {")
+        w("        const int kq = fastdiv ? (int)(((unsigned long long)k * njinv) >> 32) : k / nj;")
+        w("        const int i = c.bi0 + kq, j = c.kj0 + (k - kq * nj);")
+        w("        const BraPrim bp = load_bra_prim(c, i);")
+        w("        if(c.check && bp.skip) continue;")
+        w("        {")
+    else:
+        w("    for(int i = c.bi0; i < c.bi1; ++i)")
+        w("    {")
+        w("        const BraPrim bp = load_bra_prim(c, i);")
+        w("        if(c.check && bp.skip) continue;")
+        w("        for(int j = c.kj0; j < c.kj1; ++j)")
+        w("        {")
     w("            PrimSetup s;")
     w("            if(!prim_setup(c, bp, j, s)) continue;")
     w("            double F[%d];" % (L + 1))
@@ -190,6 +208,15 @@ def emit_class(am, prec="f64"):
         w("            }")
     w("        }")
     w("    }")
+    if warp:
+        # butterfly sums over the warp (every lane ends with the totals)
+        w("    #pragma unroll")
+        w("    for(int sh = 16; sh > 0; sh >>= 1)")
+        w("    {")
+        for k in range(ntop):
+            w("        acc%d += __shfl_xor_sync(0xffffffffu, acc%d, sh);" % (k, k))
+        w("    }")
+        w("    if(lane != 0) return;")
     # HRR
     hn = {}
     for q, rule in hrr:

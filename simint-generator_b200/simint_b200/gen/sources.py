@@ -1,9 +1,10 @@
 """Write the generated CUDA sources (one file per unique AM class).
 
 Each file holds the straight-line device function of one unique class (see
-emit.py) in its FP64 and mixed variants and the __global__ wrappers for the
-two task modes (rectangle of simint_compute_eri, explicit task list of the
-batched sweep), plus a registration function.  A registry file lists them.
+emit.py) in its FP64 and mixed variants, thread-per-quartet and
+warp-per-quartet, the __global__ wrappers for the task modes (rectangle of
+simint_compute_eri, explicit task list, screened sweep), plus a registration
+function.  A registry file lists them.
 """
 
 import itertools
@@ -33,7 +34,9 @@ def kernel_file(am):
     p = class_plan(*am)
     src64, fn64, ntop = emit_class(am, "f64")
     srcmx, fnmx, _ = emit_class(am, "mixed")
-    o = [HEADER, src64, srcmx]
+    src64w, fn64w, _ = emit_class(am, "f64", warp=True)
+    srcmxw, fnmxw, _ = emit_class(am, "mixed", warp=True)
+    o = [HEADER, src64, srcmx, src64w, srcmxw]
     o.append("template<int MODE, int PREC>")
     o.append("__global__ void __launch_bounds__(128) k_%s(const KernArgs a)" % name)
     o.append("{")
@@ -48,10 +51,26 @@ def kernel_file(am):
     o.append("    else %s<true>(c, a.out + off);" % fnmx)
     o.append("}")
     o.append("")
+    # warp-per-quartet wrappers (rectangle and screened-sweep modes)
+    o.append("template<int MODE, int PREC>")
+    o.append("__global__ void __launch_bounds__(128) kw_%s(const KernArgs a)" % name)
+    o.append("{")
+    o.append("    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;")
+    o.append("    int iP, iQ; long long off;")
+    o.append("    if(!task_of<MODE>(a, t, iP, iQ, off)) return;")
+    o.append("    QuartetCtx c;")
+    o.append("    make_ctx(a, iP, iQ, c);")
+    o.append("    if(PREC == 1) { c.gL = %d; c.gamp = hrr_amp(c, %d, %d); }"
+             % (p.L, min(am[0], am[1]), min(am[2], am[3])))
+    o.append("    if(PREC == 0) %s<false>(c, a.out + off);" % fn64w)
+    o.append("    else %s<true>(c, a.out + off);" % fnmxw)
+    o.append("}")
+    o.append("")
     o.append("void register_%s(KernelTable & t)" % name)
     o.append("{")
     o.append("    ClassKernels k = {{%d, %d, %d, %d}, %d, %d, %d, %d," % (am + (p.L, ntop, p.vrr_flops(), p.hrr_flops())))
-    o.append("        {{k_%s<0,0>, k_%s<0,1>}, {k_%s<1,0>, k_%s<1,1>}, {k_%s<2,0>, k_%s<2,1>}}};" % ((name,) * 6))
+    o.append("        {{k_%s<0,0>, k_%s<0,1>}, {k_%s<1,0>, k_%s<1,1>}, {k_%s<2,0>, k_%s<2,1>}}," % ((name,) * 6))
+    o.append("        {{kw_%s<0,0>, kw_%s<0,1>}, {nullptr, nullptr}, {kw_%s<2,0>, kw_%s<2,1>}}};" % ((name,) * 4))
     o.append("    t.add(k);")
     o.append("}")
     return "\n".join(o) + "\n"
