@@ -27,8 +27,8 @@
 // destination directly; deriv=1 components are formed by translational
 // invariance (OSTEIDeriv1_Writer.cpp:334-537).
 //
-// Variants: 256 or 128 threads per CTA, B = 1, 2 or 4 (variant codes
-// 20+B and 40+B).
+// Variants: 256, 128 or 64 threads per CTA, B = 1, 2 or 4 (variant codes
+// 20+B, 40+B and 60+B).
 
 #include <cuda_runtime.h>
 #include <algorithm>
@@ -396,7 +396,7 @@ __device__ __forceinline__ void c2_batch(const C2Params & p, T * __restrict__ wa
 }
 
 template<int MODE, int NT, int DERIV, bool MIXED>
-__global__ void __launch_bounds__(NT, NT == 128 ? 4 : 2) k_coop2(const KernArgs a, const C2Params p,
+__global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT == 128 ? 4 : 2)) k_coop2(const KernArgs a, const C2Params p,
                                                                  double * __restrict__ gres)
 {
     extern __shared__ __align__(16) double sm[];
@@ -657,8 +657,11 @@ static int c2_stepdir(int i, int j, int k)
     return -1;
 }
 
-static bool c2_is_variant(int v) { return v == 21 || v == 22 || v == 24 || v == 41 || v == 42 || v == 44; }
-static int c2_threads(int v) { return v >= 40 ? 128 : 256; }
+static bool c2_is_variant(int v)
+{
+    return v == 21 || v == 22 || v == 24 || v == 41 || v == 42 || v == 44 || v == 61 || v == 62 || v == 64;
+}
+static int c2_threads(int v) { return v >= 60 ? 64 : (v >= 40 ? 128 : 256); }
 
 struct C2ItemHost
 {
@@ -1002,7 +1005,7 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
     // HRR buffers: intermediate layers (not the first, which reads the
     // accumulators, nor the last, which writes its destination) ping-pong in
     // two buffers; the bra side's result (ab|f) for all columns sits in mid
-    int hl = 0, midmax = 0;
+    int hl = 0, midmax = 0, maxslm = 0;
     for(int t = 0; t < p.ntarget; t++)
     {
         const int * tt = p.tgt[t];
@@ -1019,7 +1022,10 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
         hl = std::max(hl, side(p.brastep_j, tt[0], tt[1], ncol));
         hl = std::max(hl, side(p.ketstep_l, tt[2], tt[3], nbra));
         midmax = std::max(midmax, nbra * ncol);
+        maxslm = std::max(maxslm, std::max(p.brastep_j ? tt[1] : tt[0], p.ketstep_l ? tt[3] : tt[2]));
     }
+    // one intermediate buffer suffices up to two transfer steps per side
+    const int nbuf = maxslm >= 3 ? 2 : (maxslm == 2 ? 1 : 0);
     p.hrr_layer = (hl + 1) & ~1;
     // prepared primitive quartet: FP64 coefficients and Boys values, then an
     // FP32 copy of the coefficients (25 floats) for the mixed-precision VRR
@@ -1031,9 +1037,9 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
     for(;;)
     {
         const int waves = 3 * p.B * p.wsize;
-        const int hrr = 2 * p.hrr_layer + midmax;
+        const int hrr = nbuf * p.hrr_layer + midmax;
         p.off_hrr_b = 0;
-        p.off_hrr_mid = 2 * p.hrr_layer;
+        p.off_hrr_mid = nbuf * p.hrr_layer;
         p.off_acc = (std::max(waves, hrr) + 1) & ~1;
         p.off_prep = (p.off_acc + p.acc_size + 1) & ~1;
         p.off_surv = p.off_prep + C2_SETUP * p.prep_stride;
@@ -1158,6 +1164,17 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
     a.oidx = nullptr;
     // the FP32 VRR applies to deriv 0 in mixed mode with a positive gate
     const bool mixed = prec == SIMINT_B200_PREC_MIXED && a.gate > 0.0 && deriv == 0;
+    if(h->nthreads == 64)
+    {
+        if(deriv)
+            return mode == 0 ? c2_launch<0, 64, 1, false>(a, p, stream)
+                 : mode == 1 ? c2_launch<1, 64, 1, false>(a, p, stream) : c2_launch<2, 64, 1, false>(a, p, stream);
+        if(mixed)
+            return mode == 0 ? c2_launch<0, 64, 0, true>(a, p, stream)
+                 : mode == 1 ? c2_launch<1, 64, 0, true>(a, p, stream) : c2_launch<2, 64, 0, true>(a, p, stream);
+        return mode == 0 ? c2_launch<0, 64, 0, false>(a, p, stream)
+             : mode == 1 ? c2_launch<1, 64, 0, false>(a, p, stream) : c2_launch<2, 64, 0, false>(a, p, stream);
+    }
     if(h->nthreads == 128)
     {
         if(deriv)

@@ -1020,10 +1020,12 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
             break;
         case 21: case 22: case 24:
         case 41: case 42: case 44:
+        case 61: case 62: case 64:
             ok = coop2_supported(am, deriv, variant);
             break;
         case 121: case 122: case 124:
         case 141: case 142: case 144:
+        case 161: case 162: case 164:
             ok = prec == SIMINT_B200_PREC_MIXED && coop2_supported(am, deriv, variant - 100);
             break;
         default:

@@ -89,7 +89,7 @@ int launch_generic(KernArgs & a, const int req[4], const UniqueMap & u, int deri
 int ncart_of(int l);
 bool coop_supported(const int am[4], int deriv);
 // Cooperative kernel v2; v = 0 for the default plan or a variant code
-// (20 + B: 256 threads, 40 + B: 128 threads; B = 1, 2, 4).
+// (20 + B: 256 threads, 40 + B: 128 threads, 60 + B: 64 threads; B = 1, 2, 4).
 bool coop2_supported(const int am[4], int deriv, int v = 0);
 bool coop2_is_variant(int v);
 int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
@@ -98,8 +98,9 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
 // Kernel variant per (requested class, deriv, precision), chosen by the
 // autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
 // 5 straight-line in FP64 even in mixed mode, 6 (7) straight-line with a
-// warp per shell quartet (in FP64 even in mixed mode), 20+B / 40+B cooperative v2
-// with batch B and 256 / 128 threads; 100 + a cooperative code: that kernel
+// warp per shell quartet (in FP64 even in mixed mode), 20+B / 40+B / 60+B
+// cooperative v2 with batch B and 256 / 128 / 64 threads; 100 + a cooperative
+// code: that kernel
 // in FP64 even in mixed mode.
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5,
        VAR_WARP = 6, VAR_WARP64 = 7 };

@@ -18,7 +18,7 @@ from _util import class_shells, oracle_pairs, oracle_eri, parity_bad
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [sb.VAR_STRAIGHT, sb.VAR_STRAIGHT64, sb.VAR_WARP, sb.VAR_WARP64, 21, 22, 24, 41, 42, 44,
+VARIANTS = [sb.VAR_STRAIGHT, sb.VAR_STRAIGHT64, sb.VAR_WARP, sb.VAR_WARP64, 21, 22, 24, 41, 42, 44, 61, 62, 64,
             sb.VAR_COOP1, sb.VAR_GENERIC]
 CLASSES = [(0, 0, 0, 0), (1, 0, 1, 0), (1, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 1), (2, 2, 2, 2),
            (3, 1, 2, 1), (3, 2, 1, 0), (2, 3, 3, 0), (3, 3, 2, 2), (4, 2, 1, 1), (3, 3, 3, 3)]
