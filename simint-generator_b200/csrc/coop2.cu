@@ -335,6 +335,17 @@ __device__ __forceinline__ void c2_waves(const C2Params & p, T * __restrict__ wa
         cfd[bb] = prep + slot[bb] * PS;
         cft[bb] = (const T *)(cfd[bb] + off32);
     }
+    // the units of the next iteration are loaded one iteration (or one
+    // barrier) ahead: the tables of large classes live in L2, not L1
+    int4 q0n = make_int4(0, 0, 0, 0), q1n = q0n;
+    {
+        const int it0 = p.wstart[1] + tid, end1 = p.wstart[2];
+        if(it0 < end1)
+        {
+            q0n = __ldg(&p.items[it0]);
+            q1n = it0 + NT < end1 ? __ldg(&p.items[it0 + NT]) : q0n;
+        }
+    }
     for(int sf = 1; sf <= p.smax; sf++)
     {
         T * cur = wave + (sf % 3) * cap * W;
@@ -344,14 +355,39 @@ __device__ __forceinline__ void c2_waves(const C2Params & p, T * __restrict__ wa
         for(int it = p.wstart[sf] + tid; it < end; it += 2 * NT)
         {
             const bool two = it + NT < end;
-            const int4 q0 = __ldg(&p.items[it]);
-            const int4 q1 = two ? __ldg(&p.items[it + NT]) : q0;
+            const int4 q0 = q0n;
+            const int4 q1 = q1n;
+            {
+                // prefetch: the next iteration of this wavefront, or the
+                // first of the next wavefront
+                int nx = it + 2 * NT, ne = end;
+                if(nx >= end && sf < p.smax)
+                {
+                    nx = p.wstart[sf + 1] + tid;
+                    ne = p.wstart[sf + 2];
+                }
+                if(nx < ne)
+                {
+                    q0n = __ldg(&p.items[nx]);
+                    q1n = nx + NT < ne ? __ldg(&p.items[nx + NT]) : q0n;
+                }
+            }
             T v0[NB], v1[NB];
             c2_unit<T, NB>(q0, w1, w2, W, cft, v0);
             c2_unit<T, NB>(q1, w1, w2, W, cft, v1);
             c2_unit_store<T, NB, DERIV>(p, q0, cur, W, cfd, v0, acc);
             if(two)
                 c2_unit_store<T, NB, DERIV>(p, q1, cur, W, cfd, v1, acc);
+        }
+        if(p.wstart[sf] + tid >= end && sf < p.smax)
+        {
+            // no unit of this wavefront: fetch the first of the next one here
+            const int nx = p.wstart[sf + 1] + tid, ne = p.wstart[sf + 2];
+            if(nx < ne)
+            {
+                q0n = __ldg(&p.items[nx]);
+                q1n = nx + NT < ne ? __ldg(&p.items[nx + NT]) : q0n;
+            }
         }
         __syncthreads();
     }
