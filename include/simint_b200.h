@@ -237,6 +237,21 @@ int simint_b200_compute_eri_device(int deriv,
                                    struct simint_multi_shellpair const * Q, const void * dev_Q,
                                    double screen_tol, double * dev_integrals, void * stream);
 
+/* Fock-matrix digestion of a sweep (no counterpart in the reference, whose
+ * callers -- Psi4, GTFock -- contract the integrals themselves): from the
+ * full-layout output of simint_b200_basis_compute (dev_out of at least
+ * simint_b200_basis_output_size doubles, every shell of the basis at most
+ * the sweep's max_am), the Coulomb and exchange matrices
+ *     J_pq = sum_rs (pq|rs) D_rs,   K_pq = sum_rs (pr|qs) D_rs
+ * of a symmetric density D, all nbf x nbf row-major in device memory, basis
+ * functions shell by shell in the order given to simint_b200_basis_create
+ * and in the current Cartesian ordering inside a shell.  Quartets the sweep
+ * screened out contribute nothing.  Asynchronous on `stream`; returns the
+ * number of kernel launches or a negative SIMINT_B200_ERR_*. */
+int simint_b200_basis_nbf(simint_b200_basis const * b);
+int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
+                         const double * dev_D, double * dev_J, double * dev_K, void * stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,7 @@ struct PairClass
     std::vector<double> Q;           // Schwarz bound per pair
     std::vector<int> order;          // pair indices by decreasing Q
     const int * dorder = nullptr;
+    DevBuf dsh;                      // (sa, sb) per pair on the device (J/K digestion)
 };
 
 struct QClass
@@ -130,6 +131,8 @@ struct simint_b200_basis
     cudaStream_t own_stream = nullptr;
     // concurrent class streams of a full-layout sweep (fork/join around the
     // classes); each side stream has its own scratch workspace
+    DevBuf daooff;                          // first basis function of every shell (J/K digestion)
+    int nbf = 0;
     cudaStream_t side[SWEEP_SIDE] = {};
     cudaEvent_t fork = nullptr, join[SWEEP_SIDE] = {};
     Workspace side_ws[SWEEP_SIDE];
@@ -450,6 +453,9 @@ extern "C" void simint_b200_basis_free(simint_b200_basis * b)
     }
     for(auto & q : b->qcs)
         q.dev.release();
+    for(auto & pc : b->pcs)
+        pc.dsh.release();
+    b->daooff.release();
     b->dsums.release();
     for(int i = 0; i < SWEEP_SIDE; i++)
     {
@@ -810,4 +816,225 @@ extern "C" int simint_b200_basis_class_times(simint_b200_basis * b, int prec, do
     for(auto & e : ev)
         cudaEventDestroy(e);
     return nl;
+}
+
+
+// ---------------------------------------------------------------------
+// Fock-matrix digestion of a full-layout sweep: Coulomb and exchange
+// matrices J_pq = sum_rs (pq|rs) D_rs, K_pq = sum_rs (pr|qs) D_rs for a
+// symmetric density D, from the shell quartets the sweep computed (each
+// unordered shell pair once, each unordered pair of pairs once).  Every
+// quartet is scaled by its degeneracy (2 for a != b, 2 for c != d, 2 when
+// the bra and ket pairs differ) and adds its contributions to the raw J and
+// K; the symmetrised halves (J = (Jr + Jr^T)/4, K = (Kr + Kr^T)/8) are the
+// full sums.
+// ---------------------------------------------------------------------
+namespace {
+
+struct JKArgs
+{
+    const long long * prefix;
+    const int * border;
+    const int * korder;
+    int nb;
+    long long ntask;
+    const int2 * shX, * shY;
+    const int * aooff;
+    int na, nbb, nc, nd;
+    int same_class;                 // bra and ket pair classes equal (unique pair-pairs)
+    const double * out;
+    const double * D;
+    double * J, * K;
+    int nbf;
+};
+
+__global__ void k_jk(const JKArgs g)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= g.ntask)
+        return;
+    int lo = 0, hi = g.nb;
+    while(hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if(__ldg(g.prefix + mid) <= t) lo = mid; else hi = mid;
+    }
+    const int iP = __ldg(g.border + lo);
+    const int iQ = __ldg(g.korder + (int)(t - __ldg(g.prefix + lo)));
+    const int2 ab = g.shX[iP], cd = g.shY[iQ];
+    const double sc = (ab.x != ab.y ? 2.0 : 1.0) * (cd.x != cd.y ? 2.0 : 1.0)
+                    * ((g.same_class && iP == iQ) ? 1.0 : 2.0);
+    const int oA = g.aooff[ab.x], oB = g.aooff[ab.y], oC = g.aooff[cd.x], oD = g.aooff[cd.y];
+    const int na = g.na, nb = g.nbb, nc = g.nc, nd = g.nd, n = g.nbf;
+    const double * I = g.out + t * (long long)(na * nb * nc * nd);
+    const double * D = g.D;
+    auto v = [&](int p, int q, int r, int s) { return I[((p * nb + q) * nc + r) * nd + s] * sc; };
+    // J(p,q) += D(r,s) v ; J(r,s) += D(p,q) v
+    for(int p = 0; p < na; p++)
+        for(int q = 0; q < nb; q++)
+        {
+            double a = 0.0;
+            for(int r = 0; r < nc; r++)
+                for(int s = 0; s < nd; s++)
+                    a = fma(__ldg(D + (oC + r) * n + oD + s), v(p, q, r, s), a);
+            atomicAdd(g.J + (oA + p) * n + oB + q, a);
+        }
+    for(int r = 0; r < nc; r++)
+        for(int s = 0; s < nd; s++)
+        {
+            double a = 0.0;
+            for(int p = 0; p < na; p++)
+                for(int q = 0; q < nb; q++)
+                    a = fma(__ldg(D + (oA + p) * n + oB + q), v(p, q, r, s), a);
+            atomicAdd(g.J + (oC + r) * n + oD + s, a);
+        }
+    // K(p,r) += D(q,s) v ; K(q,s) += D(p,r) v ; K(p,s) += D(q,r) v ; K(q,r) += D(p,s) v
+    for(int p = 0; p < na; p++)
+        for(int r = 0; r < nc; r++)
+        {
+            double a = 0.0;
+            for(int q = 0; q < nb; q++)
+                for(int s = 0; s < nd; s++)
+                    a = fma(__ldg(D + (oB + q) * n + oD + s), v(p, q, r, s), a);
+            atomicAdd(g.K + (oA + p) * n + oC + r, a);
+        }
+    for(int q = 0; q < nb; q++)
+        for(int s = 0; s < nd; s++)
+        {
+            double a = 0.0;
+            for(int p = 0; p < na; p++)
+                for(int r = 0; r < nc; r++)
+                    a = fma(__ldg(D + (oA + p) * n + oC + r), v(p, q, r, s), a);
+            atomicAdd(g.K + (oB + q) * n + oD + s, a);
+        }
+    for(int p = 0; p < na; p++)
+        for(int s = 0; s < nd; s++)
+        {
+            double a = 0.0;
+            for(int q = 0; q < nb; q++)
+                for(int r = 0; r < nc; r++)
+                    a = fma(__ldg(D + (oB + q) * n + oC + r), v(p, q, r, s), a);
+            atomicAdd(g.K + (oA + p) * n + oD + s, a);
+        }
+    for(int q = 0; q < nb; q++)
+        for(int r = 0; r < nc; r++)
+        {
+            double a = 0.0;
+            for(int p = 0; p < na; p++)
+                for(int s = 0; s < nd; s++)
+                    a = fma(__ldg(D + (oA + p) * n + oD + s), v(p, q, r, s), a);
+            atomicAdd(g.K + (oB + q) * n + oC + r, a);
+        }
+}
+
+__global__ void k_jk_sym(double * __restrict__ J, double * __restrict__ K, int n)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(t >= (long long)n * n)
+        return;
+    const int i = (int)(t / n), j = (int)(t - (long long)i * n);
+    if(j < i)
+        return;
+    const double ja = J[(size_t)i * n + j], jb = J[(size_t)j * n + i];
+    const double ka = K[(size_t)i * n + j], kb = K[(size_t)j * n + i];
+    J[(size_t)i * n + j] = J[(size_t)j * n + i] = 0.25 * (ja + jb);
+    K[(size_t)i * n + j] = K[(size_t)j * n + i] = 0.125 * (ka + kb);
+}
+
+} // namespace
+
+extern "C" int simint_b200_basis_nbf(simint_b200_basis const * b)
+{
+    if(!b)
+        return SIMINT_B200_ERR_ARG;
+    int n = 0;
+    for(const auto & s : b->shells)
+        n += ncart_of(s.am);
+    return n;
+}
+
+extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
+                                    const double * dev_D, double * dev_J, double * dev_K, void * stream_)
+{
+    if(!b || !dev_out || !dev_D || !dev_J || !dev_K || dev_out_doubles < b->total_out)
+    {
+        set_error("simint_b200_basis_jk needs the full-layout output of the sweep");
+        return SIMINT_B200_ERR_ARG;
+    }
+    cudaStream_t stream = (cudaStream_t)stream_;
+    const int nbf = simint_b200_basis_nbf(b);
+    if(!b->daooff.ptr)
+    {
+        std::vector<int> off(b->shells.size());
+        int o = 0;
+        for(size_t s = 0; s < b->shells.size(); s++)
+        {
+            off[s] = o;
+            o += ncart_of(b->shells[s].am);
+        }
+        if(!b->daooff.reserve(off.size() * sizeof(int)))
+            return SIMINT_B200_ERR_CUDA;
+        cudaMemcpy(b->daooff.ptr, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice);
+        for(auto & pc : b->pcs)
+        {
+            std::vector<int2> sh(pc.sa.size());
+            for(size_t k = 0; k < sh.size(); k++)
+                sh[k] = make_int2(pc.sa[k], pc.sb[k]);
+            if(!pc.dsh.reserve(std::max<size_t>(1, sh.size()) * sizeof(int2)))
+                return SIMINT_B200_ERR_CUDA;
+            cudaMemcpy(pc.dsh.ptr, sh.data(), sh.size() * sizeof(int2), cudaMemcpyHostToDevice);
+        }
+        b->nbf = nbf;
+    }
+    // every shell must take part in the sweep (none above its max_am)
+    for(const auto & sh : b->shells)
+    {
+        bool found = false;
+        for(const auto & pc : b->pcs)
+            if(pc.la == sh.am || pc.lb == sh.am)
+                found = true;
+        if(!found)
+        {
+            set_error("a shell of the basis is above the sweep's max_am");
+            return SIMINT_B200_ERR_ARG;
+        }
+    }
+    cudaMemsetAsync(dev_J, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    cudaMemsetAsync(dev_K, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    int nl = 0;
+    for(auto & q : b->qcs)
+    {
+        if(q.ntask == 0)
+            continue;
+        KernArgs a;
+        fill_args(b, q, a);
+        JKArgs g;
+        g.prefix = a.prefix;
+        g.border = a.border;
+        g.korder = a.korder;
+        g.nb = a.nb;
+        g.ntask = q.ntask;
+        g.shX = (const int2 *)b->pcs[q.bx].dsh.ptr;
+        g.shY = (const int2 *)b->pcs[q.ky].dsh.ptr;
+        g.aooff = (const int *)b->daooff.ptr;
+        g.na = ncart_of(q.req[0]); g.nbb = ncart_of(q.req[1]); g.nc = ncart_of(q.req[2]); g.nd = ncart_of(q.req[3]);
+        g.same_class = q.bx == q.ky;
+        g.out = dev_out + q.offset;
+        g.D = dev_D;
+        g.J = dev_J;
+        g.K = dev_K;
+        g.nbf = nbf;
+        k_jk<<<(unsigned)((q.ntask + 127) / 128), 128, 0, stream>>>(g);
+        nl++;
+    }
+    const long long nn = (long long)nbf * nbf;
+    k_jk_sym<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(dev_J, dev_K, nbf);
+    count_launch(nl + 1);
+    const cudaError_t e = cudaGetLastError();
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("simint_b200_basis_jk: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    return nl + 1;
 }

@@ -268,6 +268,23 @@ class Basis:
         self.lib.simint_b200_basis_checksums(self.h, s.ctypes.data_as(_dp))
         return s[:2 * n].reshape(n, 2)
 
+    @property
+    def nbf(self):
+        self.lib.simint_b200_basis_nbf.argtypes = [C.c_void_p]
+        return self.lib.simint_b200_basis_nbf(self.h)
+
+    def jk(self, dev_out, ndoubles, dev_D, dev_J, dev_K, stream=0):
+        """Coulomb and exchange matrices of density D from a full-layout
+        sweep output (simint_b200_basis_jk); device pointers."""
+        L = self.lib
+        L.simint_b200_basis_jk.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]
+        r = L.simint_b200_basis_jk(self.h, C.c_void_p(dev_out), ndoubles, C.c_void_p(dev_D),
+                                   C.c_void_p(dev_J), C.c_void_p(dev_K), C.c_void_p(stream))
+        if r < 0:
+            raise RuntimeError("simint_b200_basis_jk failed: " + last_error())
+        return r
+
     def class_times(self, prec, dev_ptr, ndoubles, stream=0):
         n = self.lib.simint_b200_basis_nclass(self.h)
         ms = (C.c_float * max(n, 1))()
