@@ -332,6 +332,39 @@ def run_b200(args):
             big = ref > 1e-10 * float(ref.max())
             errs[k] = (float(d.max()), float((d[big] / ref[big]).max()) if bool(big.any()) else 0.0)
         del out64
+    # Fock digestion of the (mixed) sweep output: Coulomb and exchange
+    # matrices of a seeded symmetric density (simint_b200_basis_jk)
+    jk = None
+    if full:
+        nbf = B.nbf
+        g = torch.Generator(device="cpu").manual_seed(SEED)
+        Dm = torch.rand((nbf, nbf), generator=g, dtype=torch.float64) - 0.5
+        Dm = (0.5 * (Dm + Dm.T)).cuda()
+        Jm = torch.empty_like(Dm)
+        Km = torch.empty_like(Dm)
+        B.jk(out.data_ptr(), cap, Dm.data_ptr(), Jm.data_ptr(), Km.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        jms = []
+        for _ in range(3):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            B.jk(out.data_ptr(), cap, Dm.data_ptr(), Jm.data_ptr(), Km.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            jms.append(e0.elapsed_time(e1))
+        jt = statistics.median(jms)
+        nq = sum(c["nquart"] for c in classes)
+        ob = B.output_size * 8
+        hbm = None
+        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(mp):
+            hbm = json.load(open(mp)).get("hbm_gbs")
+        jk = {"ms": jt, "quartets_s": nq / jt * 1e3, "integrals_gb_s": ob / jt / 1e6, "nbf": nbf,
+              "hbm_frac": (ob / jt / 1e6) / hbm if hbm else None,
+              "note": "J and K of a seeded symmetric density from the sweep sample's integrals "
+                      "(reads every integral once from HBM; fraction of the measured copy bandwidth)"}
+        del Dm, Jm, Km
     total_npq = npq
     if dist:
         from simint_b200.shard import reduce_count_sum
@@ -424,7 +457,7 @@ def run_b200(args):
                          "peak_source": "measured FP64 FMA-chain probe (simint_b200_fma_peak), of measured",
                          "flop_model": "reference generator op counts per unique class (simint_b200.perfmodel)",
                          "fp32_peak": peak32},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "fock_jk": jk,
             "clocks": clkmx, "clocks_fp64": clk64, "per_class": per_class,
         }
         print(json.dumps(res))

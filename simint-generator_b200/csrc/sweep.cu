@@ -848,9 +848,16 @@ struct JKArgs
     int nbf;
 };
 
-__global__ void k_jk(const JKArgs g)
+// One warp per shell quartet: the quartet's integrals are staged in shared
+// memory (coalesced), then each of the six contractions gives every lane
+// outer elements (p,q), (r,s), ... to sum over the inner pair; one atomic
+// add per outer element.
+template<int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double jsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * WPB + warp;
     if(t >= g.ntask)
         return;
     int lo = 0, hi = g.nb;
@@ -866,65 +873,70 @@ __global__ void k_jk(const JKArgs g)
                     * ((g.same_class && iP == iQ) ? 1.0 : 2.0);
     const int oA = g.aooff[ab.x], oB = g.aooff[ab.y], oC = g.aooff[cd.x], oD = g.aooff[cd.y];
     const int na = g.na, nb = g.nbb, nc = g.nc, nd = g.nd, n = g.nbf;
-    const double * I = g.out + t * (long long)(na * nb * nc * nd);
+    const int nout = na * nb * nc * nd;
+    double * I = jsm + (size_t)warp * nout;
+    const double * src = g.out + t * (long long)nout;
+    for(int k = lane; k < nout; k += 32)
+        I[k] = __ldg(src + k) * sc;
+    __syncwarp();
     const double * D = g.D;
-    auto v = [&](int p, int q, int r, int s) { return I[((p * nb + q) * nc + r) * nd + s] * sc; };
-    // J(p,q) += D(r,s) v ; J(r,s) += D(p,q) v
-    for(int p = 0; p < na; p++)
+    // J(p,q) += sum_rs D(r,s) I ; J(r,s) += sum_pq D(p,q) I
+    for(int e = lane; e < na * nb; e += 32)
+    {
+        const int p = e / nb, q = e - p * nb;
+        const double * row = I + e * nc * nd;
+        double a = 0.0;
+        for(int r = 0; r < nc; r++)
+            for(int s2 = 0; s2 < nd; s2++)
+                a = fma(__ldg(D + (oC + r) * n + oD + s2), row[r * nd + s2], a);
+        atomicAdd(g.J + (oA + p) * n + oB + q, a);
+    }
+    for(int e = lane; e < nc * nd; e += 32)
+    {
+        const int r = e / nd, s2 = e - r * nd;
+        double a = 0.0;
+        for(int p = 0; p < na; p++)
+            for(int q = 0; q < nb; q++)
+                a = fma(__ldg(D + (oA + p) * n + oB + q), I[(p * nb + q) * nc * nd + e], a);
+        atomicAdd(g.J + (oC + r) * n + oD + s2, a);
+    }
+    // K(p,r) += D(q,s) I ; K(q,s) += D(p,r) I ; K(p,s) += D(q,r) I ; K(q,r) += D(p,s) I
+    for(int e = lane; e < na * nc; e += 32)
+    {
+        const int p = e / nc, r = e - p * nc;
+        double a = 0.0;
         for(int q = 0; q < nb; q++)
-        {
-            double a = 0.0;
+            for(int s2 = 0; s2 < nd; s2++)
+                a = fma(__ldg(D + (oB + q) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
+        atomicAdd(g.K + (oA + p) * n + oC + r, a);
+    }
+    for(int e = lane; e < nb * nd; e += 32)
+    {
+        const int q = e / nd, s2 = e - q * nd;
+        double a = 0.0;
+        for(int p = 0; p < na; p++)
             for(int r = 0; r < nc; r++)
-                for(int s = 0; s < nd; s++)
-                    a = fma(__ldg(D + (oC + r) * n + oD + s), v(p, q, r, s), a);
-            atomicAdd(g.J + (oA + p) * n + oB + q, a);
-        }
-    for(int r = 0; r < nc; r++)
-        for(int s = 0; s < nd; s++)
-        {
-            double a = 0.0;
-            for(int p = 0; p < na; p++)
-                for(int q = 0; q < nb; q++)
-                    a = fma(__ldg(D + (oA + p) * n + oB + q), v(p, q, r, s), a);
-            atomicAdd(g.J + (oC + r) * n + oD + s, a);
-        }
-    // K(p,r) += D(q,s) v ; K(q,s) += D(p,r) v ; K(p,s) += D(q,r) v ; K(q,r) += D(p,s) v
-    for(int p = 0; p < na; p++)
-        for(int r = 0; r < nc; r++)
-        {
-            double a = 0.0;
-            for(int q = 0; q < nb; q++)
-                for(int s = 0; s < nd; s++)
-                    a = fma(__ldg(D + (oB + q) * n + oD + s), v(p, q, r, s), a);
-            atomicAdd(g.K + (oA + p) * n + oC + r, a);
-        }
-    for(int q = 0; q < nb; q++)
-        for(int s = 0; s < nd; s++)
-        {
-            double a = 0.0;
-            for(int p = 0; p < na; p++)
-                for(int r = 0; r < nc; r++)
-                    a = fma(__ldg(D + (oA + p) * n + oC + r), v(p, q, r, s), a);
-            atomicAdd(g.K + (oB + q) * n + oD + s, a);
-        }
-    for(int p = 0; p < na; p++)
-        for(int s = 0; s < nd; s++)
-        {
-            double a = 0.0;
-            for(int q = 0; q < nb; q++)
-                for(int r = 0; r < nc; r++)
-                    a = fma(__ldg(D + (oB + q) * n + oC + r), v(p, q, r, s), a);
-            atomicAdd(g.K + (oA + p) * n + oD + s, a);
-        }
-    for(int q = 0; q < nb; q++)
-        for(int r = 0; r < nc; r++)
-        {
-            double a = 0.0;
-            for(int p = 0; p < na; p++)
-                for(int s = 0; s < nd; s++)
-                    a = fma(__ldg(D + (oA + p) * n + oD + s), v(p, q, r, s), a);
-            atomicAdd(g.K + (oB + q) * n + oC + r, a);
-        }
+                a = fma(__ldg(D + (oA + p) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
+        atomicAdd(g.K + (oB + q) * n + oD + s2, a);
+    }
+    for(int e = lane; e < na * nd; e += 32)
+    {
+        const int p = e / nd, s2 = e - p * nd;
+        double a = 0.0;
+        for(int q = 0; q < nb; q++)
+            for(int r = 0; r < nc; r++)
+                a = fma(__ldg(D + (oB + q) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
+        atomicAdd(g.K + (oA + p) * n + oD + s2, a);
+    }
+    for(int e = lane; e < nb * nc; e += 32)
+    {
+        const int q = e / nc, r = e - q * nc;
+        double a = 0.0;
+        for(int p = 0; p < na; p++)
+            for(int s2 = 0; s2 < nd; s2++)
+                a = fma(__ldg(D + (oA + p) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
+        atomicAdd(g.K + (oB + q) * n + oC + r, a);
+    }
 }
 
 __global__ void k_jk_sym(double * __restrict__ J, double * __restrict__ K, int n)
@@ -1024,7 +1036,25 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
         g.J = dev_J;
         g.K = dev_K;
         g.nbf = nbf;
-        k_jk<<<(unsigned)((q.ntask + 127) / 128), 128, 0, stream>>>(g);
+        // the quartet's integrals are staged per warp: 4 warps per block
+        // while they fit 96 KB, else 1 (classes up to 25 600 integrals per
+        // shell quartet, e.g. (gg|dd))
+        const size_t per_warp = (size_t)q.nout * sizeof(double);
+        if(per_warp > 200 * 1024)
+        {
+            set_error("simint_b200_basis_jk: class too large for the digestion kernel");
+            return SIMINT_B200_ERR_CLASS;
+        }
+        if(4 * per_warp <= 96 * 1024)
+        {
+            cudaFuncSetAttribute(k_jk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+            k_jk<4><<<(unsigned)((q.ntask + 3) / 4), 128, 4 * per_warp, stream>>>(g);
+        }
+        else
+        {
+            cudaFuncSetAttribute(k_jk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            k_jk<1><<<(unsigned)q.ntask, 32, per_warp, stream>>>(g);
+        }
         nl++;
     }
     const long long nn = (long long)nbf * nbf;
