@@ -365,6 +365,36 @@ def run_b200(args):
               "note": "J and K of a seeded symmetric density from the sweep sample's integrals "
                       "(reads every integral once from HBM; fraction of the measured copy bandwidth)"}
         del Dm, Jm, Km
+    # one-electron matrices of the same basis (simint_b200_oei_matrix):
+    # overlap, kinetic energy and the nuclear attraction of the workload's
+    # pseudo-atoms (distinct shell centres) as point charges Z = 6
+    oei = None
+    if full:
+        atoms = np.unique(np.array([[S.arr[i].x, S.arr[i].y, S.arr[i].z] for i in range(S.n)]), axis=0)
+        cen = np.concatenate([atoms, np.full((len(atoms), 1), 6.0)], axis=1)
+        nbf = B.nbf
+        M = torch.empty((nbf, nbf), dtype=torch.float64, device="cuda")
+        npp = sum(S.arr[i].nprim * S.arr[j].nprim for i in range(S.n) for j in range(i + 1))
+        oei = {"nbf": nbf, "ncentre": len(atoms), "shell_pairs": S.n * (S.n + 1) // 2,
+               "primitive_pairs": npp,
+               "note": "overlap, kinetic and nuclear-attraction matrices of the basis (every unique "
+                       "shell pair, both triangles written); potential over the pseudo-atoms, Z = 6"}
+        for kind, name in ((sb.OEI_OVERLAP, "overlap"), (sb.OEI_KINETIC, "kinetic"),
+                           (sb.OEI_POTENTIAL, "potential")):
+            sb.oei_matrix(kind, S, cen, M.data_ptr(), stream.cuda_stream, lib)
+            torch.cuda.synchronize()
+            t = []
+            for _ in range(3):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                sb.oei_matrix(kind, S, cen, M.data_ptr(), stream.cuda_stream, lib)
+                e1.record(stream)
+                e1.synchronize()
+                t.append(e0.elapsed_time(e1))
+            oei[name + "_ms"] = statistics.median(t)
+        oei["potential_items_s"] = npp * len(atoms) / oei["potential_ms"] * 1e3
+        del M
     total_npq = npq
     if dist:
         from simint_b200.shard import reduce_count_sum
@@ -457,7 +487,7 @@ def run_b200(args):
                          "peak_source": "measured FP64 FMA-chain probe (simint_b200_fma_peak), of measured",
                          "flop_model": "reference generator op counts per unique class (simint_b200.perfmodel)",
                          "fp32_peak": peak32},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "fock_jk": jk,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "fock_jk": jk, "one_electron": oei,
             "clocks": clkmx, "clocks_fp64": clk64, "per_class": per_class,
         }
         print(json.dumps(res))

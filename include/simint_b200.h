@@ -254,6 +254,24 @@ int simint_b200_basis_nbf(simint_b200_basis const * b);
 int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
                          const double * dev_D, double * dev_J, double * dev_K, void * stream);
 
+/* One-electron matrices of a whole basis (the batched form of
+ * simint_compute_overlap / simint_compute_ke / simint_compute_potential,
+ * skel/simint/simint_oneelectron.h:12-27): kind SIMINT_B200_OEI_OVERLAP,
+ * _KINETIC or _POTENTIAL (-sum_C Z_C 1/|r - C| over the ncenter point
+ * charges Z, x, y, z, host arrays).  Writes the full symmetric nbf x nbf
+ * matrix, row-major, into dev_out (device memory): basis functions shell by
+ * shell in the given order, Cartesians inside a shell in the current ERI
+ * ordering (simint_b200_set_ordering), so the matrix pairs with the
+ * sweep's J and K.  Every shell at most am 4.  Asynchronous on `stream`
+ * (the shells and centres are copied before the call returns); returns the
+ * number of kernel launches or a negative SIMINT_B200_ERR_*. */
+#define SIMINT_B200_OEI_OVERLAP   0
+#define SIMINT_B200_OEI_KINETIC   1
+#define SIMINT_B200_OEI_POTENTIAL 2
+int simint_b200_oei_matrix(int kind, int nshell, struct simint_shell const * shells,
+                           int ncenter, const double * Z, const double * x, const double * y,
+                           const double * z, double * dev_out, void * stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,13 +2,15 @@
 
 TEST INFRASTRUCTURE ONLY.
 
-* oracle/liboracle.so   <- oracle/ostei_oracle.c (our C restatement), plain
+* oracle/liboracle.so   <- oracle/ostei_oracle.c + osoei_oracle.c (our C
+  restatements of the two- and one-electron integrals), plain
   gcc -O2, plus an OpenMP driver used only as the timed CPU baseline.
 * oracle/_ref/libsimint_ref.so <- compiled straight from the reference's
   sources where they lie (no reference build system is run):
     skel/simint/shell/shell.c, shell_screen.c, shell_constants.c
         (pair precompute, normalisation, screening),
     skel/simint/boys/boys_shortgrid.c + boys.h (Boys grid and evaluation),
+    skel/simint/osoei/osoei_*.c + recur_lookup.c (one-electron integrals),
     skel/test/ValeevRef.cpp (the reference's own long-double test oracle),
   with small glue files from oracle/ (ref_shim*.c*) and two configuration
   headers that the reference's CMake would otherwise generate
@@ -46,18 +48,20 @@ def build_oracle_ld(force=False):
     double-precision error of ill-conditioned elements."""
     _ensure_boys()
     out = os.path.join(HERE, "liboracle_ld.so")
-    src = os.path.join(HERE, "ostei_oracle.c")
-    if not force and os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+    srcs = [os.path.join(HERE, "ostei_oracle.c"), os.path.join(HERE, "osoei_oracle.c")]
+    if not force and os.path.exists(out) and all(
+            os.path.getmtime(out) >= os.path.getmtime(s) for s in srcs):
         return out
     _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu11", "-DORACLE_LONG_DOUBLE",
-          "-I", os.path.join(REPO, "include"), "-I", GEN, "-o", out, src, "-lm"])
+          "-I", os.path.join(REPO, "include"), "-I", GEN, "-o", out] + srcs + ["-lm"])
     return out
 
 
 def build_oracle(force=False):
     _ensure_boys()
     out = os.path.join(HERE, "liboracle.so")
-    srcs = [os.path.join(HERE, "ostei_oracle.c"), os.path.join(HERE, "oracle_omp.c")]
+    srcs = [os.path.join(HERE, "ostei_oracle.c"), os.path.join(HERE, "osoei_oracle.c"),
+            os.path.join(HERE, "oracle_omp.c")]
     if not force and os.path.exists(out) and all(
             os.path.getmtime(out) >= os.path.getmtime(s) for s in srcs):
         return out
@@ -137,6 +141,11 @@ def build_ref(force=False):
         cc(os.path.join(skel, "simint", f), inc8)
     cc(os.path.join(skel, "simint", "boys", "boys_shortgrid.c"), inc1, extra=["-DSIMINT_SCALAR"])
     cc(os.path.join(HERE, "ref_shim_boys.c"), inc1, extra=["-DSIMINT_SCALAR"])
+    # one-electron integrals (overlap, kinetic energy, nuclear attraction)
+    # and the Cartesian lookup table they index through
+    for f in ("osoei/osoei_overlap.c", "osoei/osoei_ke.c", "osoei/osoei_potential.c",
+              "osoei/osoei_terms.c", "recur_lookup.c"):
+        cc(os.path.join(skel, "simint", f), inc1, extra=["-DSIMINT_SCALAR"])
     cc(os.path.join(skel, "test", "ValeevRef.cpp"), inc8, lang="c++")
     cc(os.path.join(HERE, "ref_shim.cpp"), inc8, lang="c++")
     cc(os.path.join(HERE, "ref_shim_eri.c"), inc8)

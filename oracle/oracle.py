@@ -42,6 +42,10 @@ def load_oracle():
     lib.oracle_bench_rows.argtypes = [C.c_int, C.POINTER(PairP), C.POINTER(PairP), C.c_double,
                                       C.c_int, C.POINTER(C.c_longlong), _dp]
     lib.oracle_bench_rows.restype = C.c_double
+    lib.oracle_oei_st.argtypes = [C.c_int, ShellP, ShellP, _dp]
+    lib.oracle_oei_st.restype = C.c_int
+    lib.oracle_oei_potential.argtypes = [C.c_int, _dp, _dp, _dp, _dp, ShellP, ShellP, _dp]
+    lib.oracle_oei_potential.restype = C.c_int
     return lib
 
 
@@ -55,6 +59,11 @@ def load_oracle_ld():
     lib = C.CDLL(path)
     lib.oracle_compute_eri.argtypes = [PairP, PairP, C.c_double, C.c_int, C.c_int, C.c_void_p]
     lib.oracle_compute_eri.restype = C.c_int
+    # one-electron integrals: evaluated in long double, rounded to double
+    lib.oracle_oei_st.argtypes = [C.c_int, ShellP, ShellP, _dp]
+    lib.oracle_oei_st.restype = C.c_int
+    lib.oracle_oei_potential.argtypes = [C.c_int, _dp, _dp, _dp, _dp, ShellP, ShellP, _dp]
+    lib.oracle_oei_potential.restype = C.c_int
     return lib
 
 
@@ -74,4 +83,9 @@ def load_ref():
     lib.ref_boys_grid.restype = C.c_double
     lib.ref_boys_longfac.argtypes = [C.c_int]
     lib.ref_boys_longfac.restype = C.c_double
+    for f in ("simint_compute_osoei_overlap", "simint_compute_osoei_ke"):
+        getattr(lib, f).argtypes = [ShellP, ShellP, _dp]
+        getattr(lib, f).restype = C.c_int
+    lib.simint_compute_osoei_potential.argtypes = [C.c_int, _dp, _dp, _dp, _dp, ShellP, ShellP, _dp]
+    lib.simint_compute_osoei_potential.restype = C.c_int
     return lib

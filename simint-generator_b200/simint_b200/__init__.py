@@ -87,6 +87,49 @@ def make_pairs(lib, shells, pairs, screen=SIMINT_SCREEN_NONE):
     return P
 
 
+OEI_OVERLAP, OEI_KINETIC, OEI_POTENTIAL = 0, 1, 2
+
+
+def _centres(centres):
+    """(x, y, z, Z) rows -> four contiguous arrays (kept alive by the caller)."""
+    c = np.ascontiguousarray(np.asarray(centres, float).reshape(-1, 4).T)
+    return c, [c[k].ctypes.data_as(_dp) for k in (3, 0, 1, 2)]
+
+
+def compute_oei(kind, S, a, b, centres=None, lib=None):
+    """simint_compute_overlap / _ke / _potential for shells a, b of S (the
+    reference's per-pair interface); returns (ret, block)."""
+    lib = lib or load()
+    n = ncart(S.arr[a].am) * ncart(S.arr[b].am)
+    out = np.zeros(n)
+    if kind == OEI_OVERLAP:
+        lib.simint_compute_overlap.argtypes = [ShellP, ShellP, _dp]
+        r = lib.simint_compute_overlap(S.ptr(a), S.ptr(b), out.ctypes.data_as(_dp))
+    elif kind == OEI_KINETIC:
+        lib.simint_compute_ke.argtypes = [ShellP, ShellP, _dp]
+        r = lib.simint_compute_ke(S.ptr(a), S.ptr(b), out.ctypes.data_as(_dp))
+    else:
+        keep, (Z, x, y, z) = _centres(centres if centres is not None else np.zeros((0, 4)))
+        lib.simint_compute_potential.argtypes = [C.c_int, _dp, _dp, _dp, _dp, ShellP, ShellP, _dp]
+        r = lib.simint_compute_potential(keep.shape[1], Z, x, y, z, S.ptr(a), S.ptr(b),
+                                         out.ctypes.data_as(_dp))
+    return r, out
+
+
+def oei_matrix(kind, S, centres, dev_out, stream=0, lib=None):
+    """simint_b200_oei_matrix: the nbf x nbf matrix of every shell of S into
+    device memory at dev_out; returns the launch count."""
+    lib = lib or load()
+    keep, (Z, x, y, z) = _centres(centres if centres is not None else np.zeros((0, 4)))
+    lib.simint_b200_oei_matrix.argtypes = [C.c_int, C.c_int, ShellP, C.c_int, _dp, _dp, _dp, _dp,
+                                           C.c_void_p, C.c_void_p]
+    r = lib.simint_b200_oei_matrix(kind, S.n, S.ptr(0), keep.shape[1], Z, x, y, z,
+                                   C.c_void_p(dev_out), C.c_void_p(stream))
+    if r < 0:
+        raise RuntimeError("simint_b200_oei_matrix failed: " + last_error())
+    return r
+
+
 def count_primq(P, Q, screen_tol, lib=None):
     lib = lib or load()
     lib.simint_b200_count_primq.argtypes = [PairP, PairP, C.c_double]

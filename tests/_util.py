@@ -62,3 +62,20 @@ def as_accurate_as_oracle(calc, ref, ref_ld, slack=2.0, floor=1e-14):
     e_calc = np.abs(calc.astype(np.longdouble) - ref_ld)
     e_ref = float(np.abs(ref.astype(np.longdouble) - ref_ld).max()) if ref.size else 0.0
     return np.nonzero(e_calc > slack * e_ref + floor)[0]
+
+
+def oracle_oei(orc, kind, S, a, b, centres=None):
+    """One-electron integrals of shells a, b of S from the oracle: kind 0
+    overlap, 1 kinetic energy, 2 nuclear attraction over centres (rows
+    x, y, z, Z)."""
+    dp = C.POINTER(C.c_double)
+    out = np.zeros(NC(S.arr[a].am) * NC(S.arr[b].am))
+    if kind < 2:
+        r = orc.oracle_oei_st(kind, S.ptr(a), S.ptr(b), out.ctypes.data_as(dp))
+    else:
+        c = np.ascontiguousarray(np.asarray(centres, float).T)
+        r = orc.oracle_oei_potential(c.shape[1], c[3].ctypes.data_as(dp), c[0].ctypes.data_as(dp),
+                                     c[1].ctypes.data_as(dp), c[2].ctypes.data_as(dp),
+                                     S.ptr(a), S.ptr(b), out.ctypes.data_as(dp))
+    assert r == 1
+    return out

@@ -18,6 +18,11 @@ Outputs (numpy .npz, a few hundred kB in total):
   boys_ref.npz       reference boys_F_split values and grid rows
   pairs_ref.npz      reference multi-shell-pair arrays (no screening and
                      fast Schwarz), for bit-exact checks of our pair code
+  oei_ref.npz        reference one-electron integrals (overlap, kinetic
+                     energy, nuclear attraction; skel/simint/osoei) for every
+                     (la|lb) up to (g|g)
+
+`--oei-only` regenerates oei_ref.npz alone.
 """
 
 import ctypes as C
@@ -127,10 +132,47 @@ def make_pairs(ref):
     return data
 
 
+def make_oei(ref):
+    """Reference one-electron integrals (skel/simint/osoei): overlap, kinetic
+    energy and nuclear attraction of every (la, lb) up to (g|g), two shells
+    per side (shared centres included), six point charges."""
+    rng = np.random.default_rng(777)
+    dp = C.POINTER(C.c_double)
+    data = {}
+    for la in range(5):
+        for lb in range(5):
+            shells = random_shells(rng, [la, la, lb, lb], nprim_range=(1, 4), alpha=(0.05, 5e3),
+                                   box=3.0, natom=3)
+            S = normalized(ref, shells)
+            norm = [(s[0], s[1], s[2], S.coefs(k)) for k, s in enumerate(shells)]
+            cen = rng.uniform(-1.0, 4.0, (6, 3))
+            Z = rng.integers(1, 19, 6).astype(float)
+            X, Y, Zc = (np.ascontiguousarray(cen[:, k]) for k in range(3))
+            n = NC(la) * NC(lb)
+            vals = np.zeros((3, 2, 2, n))
+            for a in range(2):
+                for b in range(2):
+                    A, B = S.ptr(a), S.ptr(2 + b)
+                    ref.simint_compute_osoei_overlap(A, B, vals[0, a, b].ctypes.data_as(dp))
+                    ref.simint_compute_osoei_ke(A, B, vals[1, a, b].ctypes.data_as(dp))
+                    ref.simint_compute_osoei_potential(6, Z.ctypes.data_as(dp), X.ctypes.data_as(dp),
+                                                       Y.ctypes.data_as(dp), Zc.ctypes.data_as(dp),
+                                                       A, B, vals[2, a, b].ctypes.data_as(dp))
+            key = "spdfg"[la] + "spdfg"[lb]
+            for k, v in shells_to_arrays(norm).items():
+                data[key + "/" + k] = v
+            data[key + "/centres"] = np.concatenate([cen, Z[:, None]], axis=1)
+            data[key + "/values"] = vals
+    return data
+
+
 def main():
     ref = load_ref()
     if ref is None:
         raise SystemExit("oracle/_ref/libsimint_ref.so missing: run python oracle/build.py here")
+    np.savez_compressed(os.path.join(HERE, "oei_ref.npz"), **make_oei(ref))
+    if "--oei-only" in sys.argv:
+        return
     d0 = list(itertools.product(range(3), repeat=4))
     np.savez_compressed(os.path.join(HERE, "valeev_deriv0.npz"),
                         **make_valeev(ref, 0, d0, (1, 2, 1, 1), (1, 2), 11))

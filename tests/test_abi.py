@@ -34,7 +34,8 @@ def test_headers_declare_the_reference_api():
     names = declared_functions()
     for n in ["simint_init", "simint_finalize", "simint_compute_eri", "simint_compute_eri_deriv",
               "simint_create_multi_shellpair", "simint_normalize_shells", "simint_eri_workmem",
-              "simint_primscreen_schwarz", "simint_cat_multi_shellpair"]:
+              "simint_primscreen_schwarz", "simint_cat_multi_shellpair", "simint_compute_overlap",
+              "simint_compute_ke", "simint_compute_potential"]:
         assert n in names
 
 

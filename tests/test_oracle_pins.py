@@ -194,3 +194,25 @@ def test_long_double_oracle_against_valeevref(orc, key):
     eld = float(np.abs(out_ld - ref).max())
     scale = float(np.abs(ref).max())
     assert eld <= e64 + 2e-16 * scale, (key, eld, e64)
+
+
+OEI = _golden("oei_ref.npz")
+
+
+@pytest.mark.parametrize("key", _classes(OEI))
+def test_oracle_one_electron_matches_reference(orc, key):
+    """Overlap, kinetic energy and nuclear attraction of the oracle against
+    the reference's own osoei code (skel/simint/osoei) on the same shells:
+    within 1e-14 of the block's largest value (the two evaluations differ
+    only in recursion direction and rounding)."""
+    from _util import oracle_oei
+    S = ShellSet(_shells(OEI, key))
+    cen = OEI[key + "/centres"]
+    ref = OEI[key + "/values"]
+    for kind in range(3):
+        for a in range(2):
+            for b in range(2):
+                out = oracle_oei(orc, kind, S, a, 2 + b, cen)
+                r = ref[kind, a, b]
+                scale = max(1.0, float(np.abs(r).max()))
+                assert np.abs(out - r).max() <= 1e-14 * scale, (key, kind, a, b, np.abs(out - r).max())
