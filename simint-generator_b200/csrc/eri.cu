@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -589,6 +590,51 @@ int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
 // chunk k+1 and the copy of chunk k-1's results into the caller's memory run
 // while the GPU uploads, computes and downloads chunk k.  Results are the
 // same as the one-shot path (each chunk's kets in primitive-count order).
+// Opt-in phase trace of the host-buffer entry points (environment variable
+// SIMINT_B200_TRACE=1): one line per simint_compute_eri call on stderr with
+// the host time spent packing pair records, waiting for the GPU (uploads,
+// kernels, downloads) and copying results into the caller's memory.
+namespace {
+struct CallTrace
+{
+    typedef std::chrono::steady_clock clk;
+    bool on;
+    clk::time_point t0;
+    double pack = 0.0, wait = 0.0, copy = 0.0;
+    CallTrace() : on(enabled()), t0(on ? clk::now() : clk::time_point()) {}
+    static bool enabled()
+    {
+        static const bool e = [] {
+            const char * v = getenv("SIMINT_B200_TRACE");
+            return v && atoi(v) != 0;
+        }();
+        return e;
+    }
+    template<typename F>
+    void time(double & acc, F && f)
+    {
+        if(!on)
+        {
+            f();
+            return;
+        }
+        const clk::time_point a = clk::now();
+        f();
+        acc += std::chrono::duration<double, std::milli>(clk::now() - a).count();
+    }
+    void report(const simint_multi_shellpair * P, const simint_multi_shellpair * Q, size_t outbytes,
+                bool pipelined) const
+    {
+        if(!on)
+            return;
+        const double tot = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+        fprintf(stderr, "simint_b200 trace: (%d %d|%d %d) bra %d ket %d out %.1f MB pipelined %d: "
+                "total %.3f ms, pack %.3f, wait %.3f, copy %.3f\n", P->am1, P->am2, Q->am1, Q->am2,
+                P->nshell12_clip, Q->nshell12_clip, outbytes / 1e6, pipelined ? 1 : 0, tot, pack, wait, copy);
+    }
+};
+} // namespace
+
 static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, const simint_multi_shellpair * Q,
                                  double screen_tol, double * integrals, int nc)
 {
@@ -618,10 +664,13 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         set_error("out of memory for a pipelined call");
         return SIMINT_B200_ERR_CUDA;
     }
+    CallTrace tr;
     char * h = (char *)w.hstage.ptr;
     char * d = (char *)w.dpair.ptr;
-    pack_pairs(P, h, LP);
-    pack_meta(Q, LQ, qstart, h + szP);
+    tr.time(tr.pack, [&] {
+        pack_pairs(P, h, LP);
+        pack_meta(Q, LQ, qstart, h + szP);
+    });
     // P, and Q's starts/counts/AB (everything after the records)
     cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream);
     cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start, cudaMemcpyHostToDevice,
@@ -665,12 +714,14 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         const int g0 = qstart[c0], g1 = c1 >= nQ ? LQ.npad : qstart[c1];
         char * hs = h + szP + szQ + (size_t)(k & 1) * slot;
         if(k >= 2)
-            cudaEventSynchronize(ev[k & 1]);           // staging slot of chunk k-2 uploaded
-        pack_records(Q, LQ.npad, g0, g1, (double *)hs);
+            tr.time(tr.wait, [&] { cudaEventSynchronize(ev[k & 1]); });   // staging slot of chunk k-2 uploaded
         const size_t recbytes = (size_t)(g1 - g0) * SB_REC * sizeof(double);
         int * kk = (int *)(hs + recbytes);
-        for(int q = c0; q < c1; q++) kk[q - c0] = q;
-        std::stable_sort(kk, kk + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+        tr.time(tr.pack, [&] {
+            pack_records(Q, LQ.npad, g0, g1, (double *)hs);
+            for(int q = c0; q < c1; q++) kk[q - c0] = q;
+            std::stable_sort(kk, kk + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+        });
         cudaMemcpyAsync(d + szP + (size_t)g0 * SB_REC * sizeof(double), hs, recbytes, cudaMemcpyHostToDevice,
                         w.stream);
         cudaMemcpyAsync(dkord + c0, kk, (size_t)(c1 - c0) * sizeof(int), cudaMemcpyHostToDevice, w.stream);
@@ -693,12 +744,15 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         cudaEventRecord(ev[2 + k], w.dstream);
         if(k >= 1)
         {
-            cudaEventSynchronize(ev[2 + k - 1]);
-            copy_out(k - 1);
+            tr.time(tr.wait, [&] { cudaEventSynchronize(ev[2 + k - 1]); });
+            tr.time(tr.copy, [&] { copy_out(k - 1); });
         }
     }
-    cudaError_t e = cudaStreamSynchronize(w.stream);
-    const cudaError_t e2 = cudaStreamSynchronize(w.dstream);
+    cudaError_t e = cudaSuccess, e2 = cudaSuccess;
+    tr.time(tr.wait, [&] {
+        e = cudaStreamSynchronize(w.stream);
+        e2 = cudaStreamSynchronize(w.dstream);
+    });
     if(e == cudaSuccess)
         e = e2;
     if(e == cudaSuccess)
@@ -710,7 +764,8 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
         return SIMINT_B200_ERR_CUDA;
     }
-    copy_out(nchunk - 1);
+    tr.time(tr.copy, [&] { copy_out(nchunk - 1); });
+    tr.report(P, Q, outbytes, true);
     return nP * nQ;
 }
 
@@ -759,10 +814,13 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         set_error("out of memory for pair data");
         return SIMINT_B200_ERR_CUDA;
     }
+    CallTrace tr;
     char * h = (char *)w.hstage.ptr;
-    pack_pairs(P, h, LP);
-    pack_pairs(Q, h + szP, LQ);
-    memcpy(h + szP + szQ, kord.data(), kord.size() * sizeof(int));
+    tr.time(tr.pack, [&] {
+        pack_pairs(P, h, LP);
+        pack_pairs(Q, h + szP, LQ);
+        memcpy(h + szP + szQ, kord.data(), kord.size() * sizeof(int));
+    });
     char * d = (char *)w.dpair.ptr;
     cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
     const PairSetDev dP = device_view(d, LP, P->screen_max);
@@ -783,7 +841,8 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     const bool staged = outbytes >= (1u << 20) && w.hout.reserve(outbytes);
     cudaMemcpyAsync(staged ? w.hout.ptr : (void *)integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost,
                     w.stream);
-    cudaError_t e = cudaStreamSynchronize(w.stream);
+    cudaError_t e = cudaSuccess;
+    tr.time(tr.wait, [&] { e = cudaStreamSynchronize(w.stream); });
     if(e == cudaSuccess)
         e = cudaGetLastError();
     if(e != cudaSuccess)
@@ -792,7 +851,8 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         return SIMINT_B200_ERR_CUDA;
     }
     if(staged)
-        parallel_copy(integrals, w.hout.ptr, outbytes);
+        tr.time(tr.copy, [&] { parallel_copy(integrals, w.hout.ptr, outbytes); });
+    tr.report(P, Q, outbytes, false);
     return (int)nquart;
 }
 
