@@ -8,10 +8,11 @@
 // block, row-major, Cartesians in the fixed lexicographic order of
 // skel/simint/recur_lookup.c (x descending, then y).
 //
-// Mapping: one warp per shell pair.  Lanes take the primitive pairs (and, for
-// the nuclear attraction, the (centre, primitive pair) items), accumulate in
-// registers and are summed with a butterfly of shuffles in a fixed order, so
-// results do not depend on scheduling.
+// Mapping: one warp per shell pair for overlap and kinetic energy, lanes over
+// the primitive pairs; one 4-warp block per shell pair for the nuclear
+// attraction, threads over the (centre, primitive pair) items.  Threads
+// accumulate in registers; warps sum with a butterfly of shuffles and the
+// warps of a block in warp order, so results do not depend on scheduling.
 //  * overlap / kinetic energy: products of the 1-D Obara-Saika tables
 //    S_d(i, j), T_d(i, j) of each primitive pair, as in the reference;
 //  * nuclear attraction: the two-centre Obara-Saika recursion of the
@@ -251,8 +252,11 @@ __global__ void __launch_bounds__(128) k_oei_v(const OeiArgs g)
     // large ones ((d|f) and up) keep runtime loops over a local-memory table,
     // which is where the table would live anyway, and compile quickly
     constexpr int UNR = NW <= 320 ? 64 : 1;
-    const int lane = threadIdx.x & 31;
-    const int t = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    // one block per shell pair: its items spread over all the block's warps
+    // (a pair has thousands of (centre, primitive pair) items, a class may
+    // have only hundreds of pairs)
+    const int t = blockIdx.x;
     if(t >= g.npair)
         return;
     const int2 pr = g.pairs[t];
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(128) k_oei_v(const OeiArgs g)
         acc[k] = 0.0;
     const int npp = ia.y * ib.y;
     const int nitem = npp * g.ncenter;
-    for(int it = lane; it < nitem; it += 32)
+    for(int it = threadIdx.x; it < nitem; it += blockDim.x)
     {
         const int c = it / npp, r = it - c * npp;
         const int i = r / ib.y, j = r - i * ib.y;
@@ -364,10 +368,21 @@ __global__ void __launch_bounds__(128) k_oei_v(const OeiArgs g)
         for(int k = 0; k < NA * NB; k++)
             acc[k] = fma(f, W[o2off(LA, LB, LA, LB) + k], acc[k]);
     }
+    // warp sums, then the warps' sums in warp order (deterministic)
     extern __shared__ double oei_sm[];
-    double * sm = oei_sm + (threadIdx.x >> 5) * (NA * NB);
-    warp_reduce_to<NA * NB>(acc, sm, lane);
-    oei_write(g, t, pr.x, pr.y, LA, LB, sm, lane);
+    warp_reduce_to<NA * NB>(acc, oei_sm + warp * (NA * NB), lane);
+    __syncthreads();
+    if(warp != 0)
+        return;
+    for(int k = lane; k < NA * NB; k += 32)
+    {
+        double v = oei_sm[k];
+        for(int w = 1; w < nwarp; w++)
+            v += oei_sm[w * (NA * NB) + k];
+        oei_sm[k] = v;
+    }
+    __syncwarp();
+    oei_write(g, t, pr.x, pr.y, LA, LB, oei_sm, lane);
 }
 
 typedef void (*OeiKern)(OeiArgs);
@@ -510,7 +525,9 @@ int oei_launch(int kind, int la, int lb, OeiArgs g, int first, int npair, cudaSt
     if(g.mode != 2)
         g.out += (long long)first * onc(la) * onc(lb);
     const int threads = 128;
-    const long long blocks = ((long long)npair * 32 + threads - 1) / threads;
+    // overlap, kinetic energy: a warp per shell pair; nuclear attraction: a
+    // block per shell pair
+    const long long blocks = kind == 2 ? npair : ((long long)npair * 32 + threads - 1) / threads;
     const size_t smem = sizeof(double) * (threads / 32) * onc(la) * onc(lb);
     k<<<(unsigned)blocks, threads, smem, stream>>>(g);
     count_launch(1);

@@ -852,14 +852,11 @@ struct JKArgs
 // memory (coalesced), then each of the six contractions gives every lane
 // outer elements (p,q), (r,s), ... to sum over the inner pair; one atomic
 // add per outer element.
-template<int WPB>
-__global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
+// Shell quartet t of a class: its position in the task list and the
+// degeneracy factor (2 for a != b, 2 for c != d, 2 when the bra and ket
+// pairs differ).
+__device__ __forceinline__ void jk_quartet(const JKArgs & g, long long t, int2 & ab, int2 & cd, double & sc)
 {
-    extern __shared__ double jsm[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * WPB + warp;
-    if(t >= g.ntask)
-        return;
     int lo = 0, hi = g.nb;
     while(hi - lo > 1)
     {
@@ -868,20 +865,21 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
     }
     const int iP = __ldg(g.border + lo);
     const int iQ = __ldg(g.korder + (int)(t - __ldg(g.prefix + lo)));
-    const int2 ab = g.shX[iP], cd = g.shY[iQ];
-    const double sc = (ab.x != ab.y ? 2.0 : 1.0) * (cd.x != cd.y ? 2.0 : 1.0)
-                    * ((g.same_class && iP == iQ) ? 1.0 : 2.0);
+    ab = g.shX[iP];
+    cd = g.shY[iQ];
+    sc = (ab.x != ab.y ? 2.0 : 1.0) * (cd.x != cd.y ? 2.0 : 1.0)
+       * ((g.same_class && iP == iQ) ? 1.0 : 2.0);
+}
+
+// The six contractions of one staged quartet I (scaled by its degeneracy),
+// output elements over threads k0, k0 + stride, ...; one atomic add each.
+__device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, const double * I, int k0, int stride)
+{
     const int oA = g.aooff[ab.x], oB = g.aooff[ab.y], oC = g.aooff[cd.x], oD = g.aooff[cd.y];
     const int na = g.na, nb = g.nbb, nc = g.nc, nd = g.nd, n = g.nbf;
-    const int nout = na * nb * nc * nd;
-    double * I = jsm + (size_t)warp * nout;
-    const double * src = g.out + t * (long long)nout;
-    for(int k = lane; k < nout; k += 32)
-        I[k] = __ldg(src + k) * sc;
-    __syncwarp();
     const double * D = g.D;
     // J(p,q) += sum_rs D(r,s) I ; J(r,s) += sum_pq D(p,q) I
-    for(int e = lane; e < na * nb; e += 32)
+    for(int e = k0; e < na * nb; e += stride)
     {
         const int p = e / nb, q = e - p * nb;
         const double * row = I + e * nc * nd;
@@ -891,7 +889,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
                 a = fma(__ldg(D + (oC + r) * n + oD + s2), row[r * nd + s2], a);
         atomicAdd(g.J + (oA + p) * n + oB + q, a);
     }
-    for(int e = lane; e < nc * nd; e += 32)
+    for(int e = k0; e < nc * nd; e += stride)
     {
         const int r = e / nd, s2 = e - r * nd;
         double a = 0.0;
@@ -901,7 +899,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
         atomicAdd(g.J + (oC + r) * n + oD + s2, a);
     }
     // K(p,r) += D(q,s) I ; K(q,s) += D(p,r) I ; K(p,s) += D(q,r) I ; K(q,r) += D(p,s) I
-    for(int e = lane; e < na * nc; e += 32)
+    for(int e = k0; e < na * nc; e += stride)
     {
         const int p = e / nc, r = e - p * nc;
         double a = 0.0;
@@ -910,7 +908,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
                 a = fma(__ldg(D + (oB + q) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oA + p) * n + oC + r, a);
     }
-    for(int e = lane; e < nb * nd; e += 32)
+    for(int e = k0; e < nb * nd; e += stride)
     {
         const int q = e / nd, s2 = e - q * nd;
         double a = 0.0;
@@ -919,7 +917,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
                 a = fma(__ldg(D + (oA + p) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oB + q) * n + oD + s2, a);
     }
-    for(int e = lane; e < na * nd; e += 32)
+    for(int e = k0; e < na * nd; e += stride)
     {
         const int p = e / nd, s2 = e - p * nd;
         double a = 0.0;
@@ -928,7 +926,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
                 a = fma(__ldg(D + (oB + q) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oA + p) * n + oD + s2, a);
     }
-    for(int e = lane; e < nb * nc; e += 32)
+    for(int e = k0; e < nb * nc; e += stride)
     {
         const int q = e / nc, r = e - q * nc;
         double a = 0.0;
@@ -937,6 +935,47 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
                 a = fma(__ldg(D + (oA + p) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oB + q) * n + oC + r, a);
     }
+}
+
+// WPB warps per block, one shell quartet per warp, the quartet's integrals
+// staged in the warp's shared memory.
+template<int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
+{
+    extern __shared__ double jsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long t = (long long)blockIdx.x * WPB + warp;
+    if(t >= g.ntask)
+        return;
+    int2 ab, cd;
+    double sc;
+    jk_quartet(g, t, ab, cd, sc);
+    const int nout = g.na * g.nbb * g.nc * g.nd;
+    double * I = jsm + (size_t)warp * nout;
+    const double * src = g.out + t * (long long)nout;
+    for(int k = lane; k < nout; k += 32)
+        I[k] = __ldg(src + k) * sc;
+    __syncwarp();
+    jk_passes(g, ab, cd, I, lane, 32);
+}
+
+// Classes whose quartet fills more than 24 KB of shared memory: one block of
+// NT threads per shell quartet (a warp alone would leave the SM with 2-4
+// warps), the six contractions spread over all NT threads.
+template<int NT>
+__global__ void __launch_bounds__(NT) k_jkb(const JKArgs g)
+{
+    extern __shared__ double jsm[];
+    const long long t = blockIdx.x;
+    int2 ab, cd;
+    double sc;
+    jk_quartet(g, t, ab, cd, sc);
+    const int nout = g.na * g.nbb * g.nc * g.nd;
+    const double * src = g.out + t * (long long)nout;
+    for(int k = threadIdx.x; k < nout; k += NT)
+        jsm[k] = __ldg(src + k) * sc;
+    __syncthreads();
+    jk_passes(g, ab, cd, jsm, threadIdx.x, NT);
 }
 
 __global__ void k_jk_sym(double * __restrict__ J, double * __restrict__ K, int n)
@@ -1036,9 +1075,10 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
         g.J = dev_J;
         g.K = dev_K;
         g.nbf = nbf;
-        // the quartet's integrals are staged per warp: 4 warps per block
-        // while they fit 96 KB, else 1 (classes up to 25 600 integrals per
-        // shell quartet, e.g. (gg|dd))
+        // the quartet's integrals are staged in shared memory: one quartet
+        // per warp, 4 warps per block, while they fit 96 KB; else one quartet
+        // per 256-thread block (classes up to 25 600 integrals per shell
+        // quartet, e.g. (gg|dd))
         const size_t per_warp = (size_t)q.nout * sizeof(double);
         if(per_warp > 200 * 1024)
         {
@@ -1052,8 +1092,8 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
         }
         else
         {
-            cudaFuncSetAttribute(k_jk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            k_jk<1><<<(unsigned)q.ntask, 32, per_warp, stream>>>(g);
+            cudaFuncSetAttribute(k_jkb<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            k_jkb<256><<<(unsigned)q.ntask, 256, per_warp, stream>>>(g);
         }
         nl++;
     }

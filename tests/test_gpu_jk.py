@@ -19,15 +19,21 @@ from _util import oracle_pairs, oracle_eri, NC
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("ordering", [0, 1])
-def test_jk_matches_full_tensor(ordering):
+# s/p/d: every class on the warp-per-quartet kernel; with f shells the
+# classes above 3 072 integrals per quartet ((fd|fd), (ff|fd), (ff|ff)) take
+# the block-per-quartet kernel
+BASES = {"spd": [0, 1, 2, 0, 1, 2, 0, 1, 2], "spdf": [0, 1, 2, 3, 3, 2]}
+
+
+@pytest.mark.parametrize("ordering,basis", [(0, "spd"), (1, "spd"), (0, "spdf"), (1, "spdf")])
+def test_jk_matches_full_tensor(ordering, basis):
     torch = pytest.importorskip("torch")
     lib = sb.load()
     lib.simint_init()
     lib.simint_b200_set_ordering(ordering)
     orc = load_oracle()
     rng = np.random.default_rng(55)
-    ams = [0, 1, 2, 0, 1, 2, 0, 1, 2]
+    ams = BASES[basis]
     shells = random_shells(rng, ams, nprim_range=(1, 3), alpha=(0.2, 20.0), box=4.0, natom=3)
     S = ShellSet(shells)
     lib.simint_normalize_shells(S.n, S.ptr(0))
@@ -51,7 +57,7 @@ def test_jk_matches_full_tensor(ordering):
     J_ref = np.einsum("pqrs,rs->pq", T, Dm)
     K_ref = np.einsum("prqs,rs->pq", T, Dm)
     # the sweep and its digestion
-    B = sb.Basis(S, 0.0, max_am=2, lib=lib)
+    B = sb.Basis(S, 0.0, max_am=max(ams), lib=lib)
     assert B.nbf == nbf
     n = B.output_size
     out = torch.empty(n, dtype=torch.float64, device="cuda")
