@@ -246,8 +246,10 @@ int simint_b200_compute_eri_device(int deriv,
  * of a symmetric density D, all nbf x nbf row-major in device memory, basis
  * functions shell by shell in the order given to simint_b200_basis_create
  * and in the current Cartesian ordering inside a shell.  Quartets the sweep
- * screened out contribute nothing.  Classes up to 25 600 integrals per shell
- * quartet (e.g. (gg|dd)); larger ones return SIMINT_B200_ERR_CLASS.
+ * screened out contribute nothing.  Classes whose integrals and six density
+ * sub-blocks fit 227 KB of shared memory (about 28 000 integrals per shell
+ * quartet: up to (gg|gd), (gf|gf), (gg|ff)); larger ones ((gg|gf), (gg|gg))
+ * return SIMINT_B200_ERR_CLASS.
  * Asynchronous on `stream`; returns the number of kernel launches or a
  * negative SIMINT_B200_ERR_*. */
 int simint_b200_basis_nbf(simint_b200_basis const * b);

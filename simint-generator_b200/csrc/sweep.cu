@@ -871,31 +871,64 @@ __device__ __forceinline__ void jk_quartet(const JKArgs & g, long long t, int2 &
        * ((g.same_class && iP == iQ) ? 1.0 : 2.0);
 }
 
-// The six contractions of one staged quartet I (scaled by its degeneracy),
-// output elements over threads k0, k0 + stride, ...; one atomic add each.
-__device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, const double * I, int k0, int stride)
+// Density sub-blocks a quartet (ab|cd) reads, staged next to its integrals:
+// D[c][d], D[a][b], D[b][d], D[a][c], D[b][c], D[a][d] (row-major, in that
+// order); jk_dsize doubles in all.
+__host__ __device__ __forceinline__ int jk_dsize(int na, int nb, int nc, int nd)
+{
+    return nc * nd + na * nb + nb * nd + na * nc + nb * nc + na * nd;
+}
+
+__device__ __forceinline__ void jk_stage_d(const JKArgs & g, int2 ab, int2 cd, double * Ds, int k0, int stride)
+{
+    const int o[4] = {g.aooff[ab.x], g.aooff[ab.y], g.aooff[cd.x], g.aooff[cd.y]};
+    const int nn[4] = {g.na, g.nbb, g.nc, g.nd};
+    // (row shell, column shell) of the six blocks: 0 = a, 1 = b, 2 = c, 3 = d
+    const int rs[6] = {2, 0, 1, 0, 1, 0}, cs[6] = {3, 1, 3, 2, 2, 3};
+    int base = 0;
+    #pragma unroll
+    for(int b = 0; b < 6; b++)
+    {
+        const int nr = nn[rs[b]], nc = nn[cs[b]], orow = o[rs[b]], ocol = o[cs[b]];
+        for(int e = k0; e < nr * nc; e += stride)
+        {
+            const int r = e / nc, c = e - r * nc;
+            Ds[base + e] = __ldg(g.D + (size_t)(orow + r) * g.nbf + ocol + c);
+        }
+        base += nr * nc;
+    }
+}
+
+// The six contractions of one staged quartet I (scaled by its degeneracy)
+// with its staged density blocks Ds, output elements over threads k0,
+// k0 + stride, ...; one atomic add each.
+__device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, const double * I,
+                                          const double * Ds, int k0, int stride)
 {
     const int oA = g.aooff[ab.x], oB = g.aooff[ab.y], oC = g.aooff[cd.x], oD = g.aooff[cd.y];
     const int na = g.na, nb = g.nbb, nc = g.nc, nd = g.nd, n = g.nbf;
-    const double * D = g.D;
+    const double * Dcd = Ds;
+    const double * Dab = Dcd + nc * nd;
+    const double * Dbd = Dab + na * nb;
+    const double * Dac = Dbd + nb * nd;
+    const double * Dbc = Dac + na * nc;
+    const double * Dad = Dbc + nb * nc;
     // J(p,q) += sum_rs D(r,s) I ; J(r,s) += sum_pq D(p,q) I
     for(int e = k0; e < na * nb; e += stride)
     {
         const int p = e / nb, q = e - p * nb;
         const double * row = I + e * nc * nd;
         double a = 0.0;
-        for(int r = 0; r < nc; r++)
-            for(int s2 = 0; s2 < nd; s2++)
-                a = fma(__ldg(D + (oC + r) * n + oD + s2), row[r * nd + s2], a);
+        for(int rs2 = 0; rs2 < nc * nd; rs2++)
+            a = fma(Dcd[rs2], row[rs2], a);
         atomicAdd(g.J + (oA + p) * n + oB + q, a);
     }
     for(int e = k0; e < nc * nd; e += stride)
     {
         const int r = e / nd, s2 = e - r * nd;
         double a = 0.0;
-        for(int p = 0; p < na; p++)
-            for(int q = 0; q < nb; q++)
-                a = fma(__ldg(D + (oA + p) * n + oB + q), I[(p * nb + q) * nc * nd + e], a);
+        for(int pq = 0; pq < na * nb; pq++)
+            a = fma(Dab[pq], I[pq * nc * nd + e], a);
         atomicAdd(g.J + (oC + r) * n + oD + s2, a);
     }
     // K(p,r) += D(q,s) I ; K(q,s) += D(p,r) I ; K(p,s) += D(q,r) I ; K(q,r) += D(p,s) I
@@ -905,7 +938,7 @@ __device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, co
         double a = 0.0;
         for(int q = 0; q < nb; q++)
             for(int s2 = 0; s2 < nd; s2++)
-                a = fma(__ldg(D + (oB + q) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
+                a = fma(Dbd[q * nd + s2], I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oA + p) * n + oC + r, a);
     }
     for(int e = k0; e < nb * nd; e += stride)
@@ -914,7 +947,7 @@ __device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, co
         double a = 0.0;
         for(int p = 0; p < na; p++)
             for(int r = 0; r < nc; r++)
-                a = fma(__ldg(D + (oA + p) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
+                a = fma(Dac[p * nc + r], I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oB + q) * n + oD + s2, a);
     }
     for(int e = k0; e < na * nd; e += stride)
@@ -923,7 +956,7 @@ __device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, co
         double a = 0.0;
         for(int q = 0; q < nb; q++)
             for(int r = 0; r < nc; r++)
-                a = fma(__ldg(D + (oB + q) * n + oC + r), I[((p * nb + q) * nc + r) * nd + s2], a);
+                a = fma(Dbc[q * nc + r], I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oA + p) * n + oD + s2, a);
     }
     for(int e = k0; e < nb * nc; e += stride)
@@ -932,13 +965,13 @@ __device__ __forceinline__ void jk_passes(const JKArgs & g, int2 ab, int2 cd, co
         double a = 0.0;
         for(int p = 0; p < na; p++)
             for(int s2 = 0; s2 < nd; s2++)
-                a = fma(__ldg(D + (oA + p) * n + oD + s2), I[((p * nb + q) * nc + r) * nd + s2], a);
+                a = fma(Dad[p * nd + s2], I[((p * nb + q) * nc + r) * nd + s2], a);
         atomicAdd(g.K + (oB + q) * n + oC + r, a);
     }
 }
 
 // WPB warps per block, one shell quartet per warp, the quartet's integrals
-// staged in the warp's shared memory.
+// and density blocks staged in the warp's shared memory.
 template<int WPB>
 __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
 {
@@ -951,12 +984,14 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
     double sc;
     jk_quartet(g, t, ab, cd, sc);
     const int nout = g.na * g.nbb * g.nc * g.nd;
-    double * I = jsm + (size_t)warp * nout;
+    double * I = jsm + (size_t)warp * (nout + jk_dsize(g.na, g.nbb, g.nc, g.nd));
+    double * Ds = I + nout;
     const double * src = g.out + t * (long long)nout;
     for(int k = lane; k < nout; k += 32)
         I[k] = __ldg(src + k) * sc;
+    jk_stage_d(g, ab, cd, Ds, lane, 32);
     __syncwarp();
-    jk_passes(g, ab, cd, I, lane, 32);
+    jk_passes(g, ab, cd, I, Ds, lane, 32);
 }
 
 // Classes whose quartet fills more than 24 KB of shared memory: one block of
@@ -971,11 +1006,13 @@ __global__ void __launch_bounds__(NT) k_jkb(const JKArgs g)
     double sc;
     jk_quartet(g, t, ab, cd, sc);
     const int nout = g.na * g.nbb * g.nc * g.nd;
+    double * Ds = jsm + nout;
     const double * src = g.out + t * (long long)nout;
     for(int k = threadIdx.x; k < nout; k += NT)
         jsm[k] = __ldg(src + k) * sc;
+    jk_stage_d(g, ab, cd, Ds, threadIdx.x, NT);
     __syncthreads();
-    jk_passes(g, ab, cd, jsm, threadIdx.x, NT);
+    jk_passes(g, ab, cd, jsm, Ds, threadIdx.x, NT);
 }
 
 __global__ void k_jk_sym(double * __restrict__ J, double * __restrict__ K, int n)
@@ -1075,12 +1112,12 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
         g.J = dev_J;
         g.K = dev_K;
         g.nbf = nbf;
-        // the quartet's integrals are staged in shared memory: one quartet
-        // per warp, 4 warps per block, while they fit 96 KB; else one quartet
-        // per 256-thread block (classes up to 25 600 integrals per shell
-        // quartet, e.g. (gg|dd))
-        const size_t per_warp = (size_t)q.nout * sizeof(double);
-        if(per_warp > 200 * 1024)
+        // the quartet's integrals and density blocks are staged in shared
+        // memory: one quartet per warp, 4 warps per block, while they fit
+        // 96 KB; else one quartet per 256-thread block, up to 227 KB (about
+        // 28 000 integrals per shell quartet: (gg|gd), (gf|gf), (gg|ff))
+        const size_t per_warp = ((size_t)q.nout + jk_dsize(g.na, g.nbb, g.nc, g.nd)) * sizeof(double);
+        if(per_warp > 227 * 1024)
         {
             set_error("simint_b200_basis_jk: class too large for the digestion kernel");
             return SIMINT_B200_ERR_CLASS;
@@ -1092,7 +1129,7 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
         }
         else
         {
-            cudaFuncSetAttribute(k_jkb<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_jkb<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
             k_jkb<256><<<(unsigned)q.ntask, 256, per_warp, stream>>>(g);
         }
         nl++;
