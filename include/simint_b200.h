@@ -132,7 +132,7 @@ int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out
 
 /* The kernel variant chosen for a requested class (0 = untuned default,
  * 1 = register kernel, 20+B / 40+B / 60+B = cooperative kernel with 256 /
- * 128 / 64 threads and batch B = 1, 2, 4). */
+ * 128 / 64 threads and batch B = 1, 2, 4, 8). */
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first

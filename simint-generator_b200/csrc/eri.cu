@@ -1078,14 +1078,14 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case VAR_COOP1:
             ok = coop_supported(am, deriv);
             break;
-        case 21: case 22: case 24:
-        case 41: case 42: case 44:
-        case 61: case 62: case 64:
+        case 21: case 22: case 24: case 28:
+        case 41: case 42: case 44: case 48:
+        case 61: case 62: case 64: case 68:
             ok = coop2_supported(am, deriv, variant);
             break;
-        case 121: case 122: case 124:
-        case 141: case 142: case 144:
-        case 161: case 162: case 164:
+        case 121: case 122: case 124: case 128:
+        case 141: case 142: case 144: case 148:
+        case 161: case 162: case 164: case 168:
             ok = prec == SIMINT_B200_PREC_MIXED && coop2_supported(am, deriv, variant - 100);
             break;
         default:

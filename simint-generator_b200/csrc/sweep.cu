@@ -658,7 +658,7 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
             if(prec == SIMINT_B200_PREC_MIXED)
                 cand.push_back(VAR_WARP64);
         }
-        for(int v : {21, 22, 24, 41, 42, 44, 61, 62, 64})
+        for(int v : {21, 22, 24, 28, 41, 42, 44, 48, 61, 62, 64, 68})
             if(coop2_supported(q.req, 0, v))
             {
                 cand.push_back(v);

@@ -160,9 +160,9 @@ def compute_eri(P, Q, screen_tol=0.0, deriv=0, lib=None):
 
 VAR_DEFAULT, VAR_STRAIGHT, VAR_COOP1, VAR_GENERIC, VAR_STRAIGHT64 = 0, 1, 3, 4, 5
 VAR_WARP, VAR_WARP64 = 6, 7                 # register kernel, one warp per shell quartet
-VAR_COOP2 = {1: 21, 2: 22, 4: 24}          # cooperative kernel, 256 threads, batch B
-VAR_COOP2_128 = {1: 41, 2: 42, 4: 44}      # cooperative kernel, 128 threads, batch B
-VAR_COOP2_64 = {1: 61, 2: 62, 4: 64}       # cooperative kernel, 64 threads, batch B
+VAR_COOP2 = {1: 21, 2: 22, 4: 24, 8: 28}          # cooperative kernel, 256 threads, batch B
+VAR_COOP2_128 = {1: 41, 2: 42, 4: 44, 8: 48}      # cooperative kernel, 128 threads, batch B
+VAR_COOP2_64 = {1: 61, 2: 62, 4: 64, 8: 68}       # cooperative kernel, 64 threads, batch B
 
 
 def get_variant(am, deriv=0, prec=0, lib=None):

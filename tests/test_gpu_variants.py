@@ -18,7 +18,8 @@ from _util import class_shells, oracle_pairs, oracle_eri, parity_bad
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [sb.VAR_STRAIGHT, sb.VAR_STRAIGHT64, sb.VAR_WARP, sb.VAR_WARP64, 21, 22, 24, 41, 42, 44, 61, 62, 64,
+VARIANTS = [sb.VAR_STRAIGHT, sb.VAR_STRAIGHT64, sb.VAR_WARP, sb.VAR_WARP64, 21, 22, 24, 28, 41, 42, 44, 48, 61, 62,
+            64, 68,
             sb.VAR_COOP1, sb.VAR_GENERIC]
 CLASSES = [(0, 0, 0, 0), (1, 0, 1, 0), (1, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 1), (2, 2, 2, 2),
            (3, 1, 2, 1), (3, 2, 1, 0), (2, 3, 3, 0), (3, 3, 2, 2), (4, 2, 1, 1), (3, 3, 3, 3)]
@@ -95,3 +96,35 @@ def test_fp64_forms_under_mixed_mode(libs, am):
         sb.set_variant(am, sb.VAR_DEFAULT, 0, sb.MIXED, lib)
         lib.simint_free_multi_shellpair(C.byref(P))
         lib.simint_free_multi_shellpair(C.byref(Q))
+
+
+@pytest.mark.parametrize("am", [(2, 1, 2, 1), (3, 2, 1, 0)], ids=["dpdp", "fdps"])
+def test_fp32_batches_agree_across_cooperative_variants(libs, am):
+    """Mixed mode with a loose gate sends most primitive quartets through the
+    FP32 batches (2B of them, at most 8, per batch); every thread count and
+    batch size must give the same integrals as batch 1 (the VRR of a
+    primitive quartet does not depend on its batch, the sums run in
+    primitive order)."""
+    lib, orc = libs
+    rng = np.random.default_rng(2718 + sum(am))
+    shells, grp = class_shells(rng, am, nsh=(2, 1, 2, 1), nprim=(3, 4), alpha=(0.3, 30.0))
+    S = ShellSet(shells)
+    orc.oracle_normalize_shells(S.n, S.ptr(0))
+    P = sb.make_pairs(lib, S, [(i, j) for i in grp[0] for j in grp[1]])
+    Q = sb.make_pairs(lib, S, [(i, j) for i in grp[2] for j in grp[3]])
+    outs = {}
+    try:
+        lib.simint_b200_set_precision(sb.MIXED, 1e-3)
+        for v in (21, 22, 24, 28, 41, 42, 44, 48, 61, 62, 64, 68):
+            if sb.set_variant(am, v, 0, sb.MIXED, lib) != 0:
+                continue
+            r, outs[v] = sb.compute_eri(P, Q, 0.0, 0, lib)
+    finally:
+        lib.simint_b200_set_precision(sb.FP64, 0.0)
+        sb.set_variant(am, sb.VAR_DEFAULT, 0, sb.MIXED, lib)
+        lib.simint_free_multi_shellpair(C.byref(P))
+        lib.simint_free_multi_shellpair(C.byref(Q))
+    assert 21 in outs and 28 in outs, sorted(outs)
+    scale = float(np.abs(outs[21]).max())
+    for v, o in outs.items():
+        assert np.abs(o - outs[21]).max() <= 1e-13 * scale, (v, np.abs(o - outs[21]).max(), scale)
