@@ -312,7 +312,7 @@ void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, do
 {
     const bool has_screen = P->screen != nullptr;
     g1 = std::min(g1, npad);
-    parallel_for((size_t)(g1 - g0 + 7) / 8, 2048, [&](size_t b0, size_t b1) {
+    parallel_for((size_t)(g1 - g0 + 7) / 8, 256, [&](size_t b0, size_t b1) {
         for(int g = g0 + (int)b0 * 8; g < std::min(g0 + (int)b1 * 8, g1); g += 8)
         {
             double m = 0.0;
@@ -642,7 +642,8 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
     const int nP = P->nshell12_clip, nQ = Q->nshell12_clip;
     const size_t outbytes = (size_t)nP * nQ * nc * sizeof(double);
     // few chunks: each launch must still fill the GPU
-    const int nch = (int)std::min<size_t>(4, std::max<size_t>(2, outbytes / ((size_t)32 << 20)));
+    const size_t moved = outbytes + (size_t)Q->nprim * SB_REC * sizeof(double);
+    const int nch = (int)std::min<size_t>(4, std::max<size_t>(2, moved / ((size_t)32 << 20)));
     const int cq = std::max(16, ((nQ + nch - 1) / nch + 15) & ~15);
     PackedLayout LP, LQ;
     std::vector<int> qstart;
@@ -798,7 +799,10 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         return 0;
     {
         const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);
-        if((size_t)nquart * nc * sizeof(double) >= ((size_t)16 << 20) && Q->nshell12_clip >= 64)
+        // pipelined when the call moves >= 16 MB (results down plus ket
+        // records up: long ket lists of small classes are upload-bound)
+        const size_t moved = (size_t)nquart * nc * sizeof(double) + (size_t)Q->nprim * SB_REC * sizeof(double);
+        if(moved >= ((size_t)16 << 20) && Q->nshell12_clip >= 64)
             return compute_eri_pipelined(deriv, P, Q, screen_tol, integrals, nc);
     }
     PackedLayout LP, LQ;
