@@ -27,7 +27,7 @@
 // destination directly; deriv=1 components are formed by translational
 // invariance (OSTEIDeriv1_Writer.cpp:334-537).
 //
-// Variants: 256, 128 or 64 threads per CTA, B = 1, 2 or 4 (variant codes
+// Variants: 256, 128 or 64 threads per CTA, B = 1, 2, 4 or 8 (variant codes
 // 20+B, 40+B and 60+B).
 
 #include <cuda_runtime.h>
