@@ -4,24 +4,31 @@
 Workload ("cfg2"): 500 seeded synthetic shells, s:p:d:f = 200:150:100:50,
 1-8 primitives, exponents log-uniform in [0.05, 5e4], 120 pseudo-atoms in a
 20 bohr cube; every shell quartet surviving the shell-pair Schwarz test
-Q_ab*Q_cd >= 1e-14, primitive screening at the same tolerance.  The full
-sweep (1.9e9 quartets, 1e11 primitive quartets) is far beyond one step, so a
-step is one pass over a proportional stratified subsample of it: every
-`--stride`-th bra-pair row of every AM class (the class mix of the whole
-sweep is kept).  Metric: evaluated primitive quartets per second.  `value`
-is the mixed-precision batched path (FP32 VRR for primitive quartets whose
-estimated FP32 error is below the gate, FP64 elsewhere); the FP64 path is
-reported beside it, with the mixed path's max absolute and relative
-deviation from it per class.
+Q_ab*Q_cd >= 1e-14, primitive screening at the same tolerance, GAMESS
+Cartesian ordering.  The full sweep (1.9e9 quartets, 1e11 primitive
+quartets) is far beyond one step, so a step is one pass over a proportional
+stratified subsample of it: every `--stride`-th bra-pair row of every AM
+class (the class mix of the whole sweep is kept).  Metric: evaluated
+primitive quartets per second.  `value` is the mixed-precision batched path
+(FP32 VRR for primitive quartets whose estimated FP32 error is below
+gate / (primitive quartets of their shell quartet), FP64 elsewhere); the
+FP64 path is reported beside it.  Both are compared element by element with
+the reference's own generated CPU library on the same quartets (max abs and
+rel error per class).
 
 Arms:
   default            B200 sweep (device-resident inputs; CUDA-graph replay),
                      plus e2e through simint_compute_eri with host buffers and
-                     the CPU oracle timed on the host cores (cpu_baseline).
-  --impl reference   the CPU restatement of the reference algorithm (the
-                     oracle; the reference's own kernels exist only as its
-                     code generator's output) on the host cores, over the
-                     same simint_compute_eri calls as e2e.
+                     the reference CPU library timed on the host cores over the
+                     same rows (cpu_baseline).
+  --impl reference   the reference's generated CPU library (create.py output,
+                     all-inline GAMESS build, gcc -O3, OpenMP over rows, all
+                     host cores) over the same sampled rows as simint_compute_eri
+                     calls (one bra pair x its surviving kets); it loads no
+                     part of the B200 library.
+
+The last stdout line is a compact JSON object; the per-class table goes to
+the file named by --detail (not printed).
 
 N > 1 (torchrun): each rank sweeps a disjoint shard of the same size as the
 one-rank sample (rows rank, rank + stride, ... of every class: weak
@@ -48,9 +55,12 @@ sys.path.insert(0, os.path.join(ROOT, "simint-generator_b200"))
 TOL = 1e-14
 MAX_AM = 3
 SEED = 2024
+GAMESS = 1
+REF_VARIANT = "gamess_l3"       # all-inline GAMESS build, max_am 3
+LINE_LIMIT = 3000               # bytes of the printed result line (kept well under 4 KB)
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -59,12 +69,17 @@ def parse():
     ap.add_argument("--stride", type=int, default=2000,
                     help="keep every stride-th bra-pair row of each class")
     ap.add_argument("--e2e-stride", type=int, default=40000)
-    ap.add_argument("--gate", type=float, default=1e-8,
-                    help="mixed precision: FP32 VRR for primitive quartets whose estimated FP32 "
-                         "error is below this (simint_b200_set_precision)")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--gate", type=float, default=1e-10,
+                    help="mixed precision: bound on the FP32 error of one integral "
+                         "(simint_b200_set_precision)")
+    ap.add_argument("--cpu-passes", type=int, default=3,
+                    help="timed passes of the reference CPU library for cpu_baseline")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the element-wise comparison with the reference library")
+    ap.add_argument("--detail", default=None,
+                    help="write the per-class table (JSON) to this file")
+    return ap.parse_args(argv)
 
 
 # ----------------------------------------------------------------------------
@@ -127,9 +142,39 @@ METRIC = "primitive quartets/s (cfg2 l<=3 screened sweep sample, screen_tol 1e-1
 def workload_config(args, world=1):
     """The workload description both arms print."""
     return {"workload": "cfg2 sweep sample: 500 shells s:p:d:f 200:150:100:50, 1-8 prims, "
-                        "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14; every %d-th bra "
-                        "row of every class per rank (rank r: rows r mod %d)" % (args.stride, args.stride),
+                        "alpha 0.05-5e4, 120 atoms in 20 bohr, Schwarz 1e-14, GAMESS order; "
+                        "every %d-th bra row of every class per rank" % args.stride,
             "parallelism": "dp%d (disjoint row shards, no data-path collective)" % world}
+
+
+def compact(res):
+    """The printed line: floats rounded to 4 significant digits, None-valued
+    keys dropped below the top level; raises past LINE_LIMIT bytes."""
+    def rnd(v):
+        if isinstance(v, float):
+            return float("%.4g" % v)
+        if isinstance(v, dict):
+            return {k: rnd(x) for k, x in v.items() if x is not None}
+        if isinstance(v, (list, tuple)):
+            return [rnd(x) for x in v]
+        return v
+    # top-level keys stay even when null (vs_baseline, cpu_baseline, ...)
+    line = json.dumps({k: rnd(v) for k, v in res.items()}, separators=(",", ":"))
+    if len(line) > LINE_LIMIT:
+        raise ValueError("result line too long (%d bytes)" % len(line))
+    return line
+
+
+def load_reference():
+    """(reflib module, refsweep module, RefLib) of the reference's generated
+    CPU library, or a reason string when it is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reflib
+    import refsweep
+    if not reflib.available(REF_VARIANT):
+        return None, None, "reference library %s not built (oracle/build_reflib.py)" % (
+            os.path.basename(reflib.lib_path(REF_VARIANT)))
+    return reflib, refsweep, reflib.load(REF_VARIANT)
 
 
 def workload_shells(lib):
@@ -138,7 +183,7 @@ def workload_shells(lib):
     shells = config_shells("cfg2")
     S = ShellSet(shells)
     lib.simint_normalize_shells(S.n, S.ptr(0))
-    return S
+    return shells, S
 
 
 def pack_bytes(P):
@@ -154,12 +199,12 @@ def e2e_rows(sb, lib, S, B, stride, rank=0):
     rows = []
     for k, c in enumerate(B.classes()):
         rr = B.rows(k)
+        sh4 = B.class_quartets(k, c["nquart"])
         for r in range(rank % stride, len(rr), stride):
             first, n = rr[r]
-            q0 = B.quartet(k, first)
-            kets = [B.quartet(k, first + i)[2:] for i in range(n)]
-            P = sb.make_pairs(lib, S, [q0[:2]], sb.SIMINT_SCREEN_SCHWARZ)
-            Q = sb.make_pairs(lib, S, kets, sb.SIMINT_SCREEN_SCHWARZ)
+            P = sb.make_pairs(lib, S, [tuple(sh4[first, :2])], sb.SIMINT_SCREEN_SCHWARZ)
+            Q = sb.make_pairs(lib, S, [tuple(x) for x in sh4[first:first + n, 2:]],
+                              sb.SIMINT_SCREEN_SCHWARZ)
             rows.append((c["am"], P, Q))
     return rows
 
@@ -169,72 +214,77 @@ def flops_of_class(am, nprimq, nquart):
     return class_flops(am, nprimq, nquart)
 
 
+def amname(am):
+    return "".join("spdfg"[x] for x in am)
+
+
 # ----------------------------------------------------------------------------
 # arms
 # ----------------------------------------------------------------------------
 
-def cpu_bench(rows, budget_s, threads):
-    """(primq/s, seconds, primq, nrows) of the oracle over a row sample that
-    takes about budget_s on `threads` host threads."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from oracle import load_oracle
-    from simint_b200.capi import PairP
-    orc = load_oracle()
-
-    def run(idx):
-        PP = (PairP * len(idx))(*[C.pointer(rows[i][1]) for i in idx])
-        QQ = (PairP * len(idx))(*[C.pointer(rows[i][2]) for i in idx])
-        npq = C.c_longlong()
-        cs = C.c_double()
-        t = orc.oracle_bench_rows(len(idx), PP, QQ, TOL, threads, C.byref(npq), C.byref(cs))
-        return t, npq.value
-
-    # interleave classes so any prefix keeps the class mix
-    idx = list(range(0, len(rows), max(1, len(rows) // 64)))[:64]
-    t, n = run(idx)
-    scale = budget_s / max(t, 1e-3)
-    take = max(1, min(len(rows), int(len(idx) * scale)))
-    step = max(1, len(rows) // take)
-    idx = list(range(0, len(rows), step))[:take]
-    t, n = run(idx)
-    return n / t, t, n, len(idx)
+def reference_rate(S, warmup, steps, threads):
+    """(primitive quartets/s, seconds per pass, primitive quartets per pass,
+    per-pass seconds) of the reference library over the sampled rows."""
+    _, prq = S.run(threads, count=True)
+    npq = int(prq.sum())
+    for _ in range(warmup):
+        S.run(threads)
+    ts = [S.run(threads)[0] for _ in range(steps)]
+    t = sum(ts) / len(ts)
+    return npq / t, t, npq, ts
 
 
 def run_reference(args):
-    import simint_b200 as sb
-    lib = sb.load()
-    lib.simint_init()
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return          # the CPU reference runs once, on rank 0
+    reflib, refsweep, R = load_reference()
+    if reflib is None:
+        print(json.dumps({"impl": "reference", "unavailable": R}))
         return
-    S = workload_shells(lib)
-    B = sb.Basis(S, TOL, MAX_AM, lib)
-    B.subsample_stride(args.stride, 0)
-    rows = e2e_rows(sb, lib, S, B, max(1, args.e2e_stride // args.stride))
+    shells = refsweep.workloads().config_shells("cfg2")
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(args.warmup):
-        cpu_bench(rows, args.cpu_seconds / 4, threads)
-    for _ in range(args.steps):
-        rate, t, n, nr = cpu_bench(rows, args.cpu_seconds, threads)
-        vals.append((rate, t, n, nr))
-    rate = statistics.median(v[0] for v in vals)
-    t = statistics.median(v[1] for v in vals)
+    S = refsweep.RefSweep(R, shells, TOL, MAX_AM, stride=args.stride, offset=0, threads=threads)
+    rate, t, npq, _ = reference_rate(S, args.warmup, args.steps, threads)
+    sample = ("%d rows (%d shell quartets, %.3g primitive quartets) of the cfg2 sweep sample, "
+              "reference %s build (create.py output, gcc -O3, OpenMP over rows)"
+              % (len(S.bh), S.nquartets, npq, REF_VARIANT))
     out = {
         "impl": "reference", "metric": METRIC,
         "value": rate, "unit": "primitive quartets/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 shells)",
-        "config": dict(workload_config(args), sample_rows=vals[-1][3], l2="n/a (CPU)",
-                       timed="simint_compute_eri-shaped rows (1 bra pair x screened kets) of the sample"),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cfg2 shells, PCG64 seed 2024)",
+        "config": dict(workload_config(args), rows=len(S.bh), l2="n/a (CPU)", setup_s=round(S.setup_s, 1),
+                       timed="simint_compute_eri per row (one bra pair x its surviving kets)"),
         "cpu_baseline": {"value": rate, "unit": "primitive quartets/s", "cores": threads,
-                         "kind": "port",
-                         "sample": "%d simint_compute_eri-shaped rows of the cfg2 sweep sample, %.3g primitive quartets"
-                                   % (vals[-1][3], vals[-1][2])},
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": rate, "unit": "primitive quartets/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(out))
+    print(compact(out))
+
+
+def check_against_reference(B, classes, outs, S, refsweep, nshell, threads):
+    """Element-wise comparison of the sweep outputs (dict name -> host array
+    in the full layout) with the reference's values for the same quartets.
+    Returns per class {name: (max abs, max rel, compared, failures)}."""
+    ref_out, _ = S.outputs(threads)
+    byam = {tuple(q["am"]): k for k, q in enumerate(S.qcs)}
+    res = []
+    for k, c in enumerate(classes):
+        kr = byam.get(tuple(c["am"]))
+        ent = {}
+        if kr is None or c["nquart"] == 0:
+            res.append(ent)
+            continue
+        keys, offs = S.class_keys(kr, nshell)
+        sh4 = B.class_quartets(k, c["nquart"])
+        a, n = c["offset"], c["nquart"] * c["nout"]
+        for name, arr in outs.items():
+            ent[name] = refsweep.compare_class(ref_out, keys, offs, arr[a:a + n], sh4, c["nout"],
+                                               nshell)
+        res.append(ent)
+    return res
 
 
 def run_b200(args):
@@ -251,7 +301,8 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lib = sb.load()
     lib.simint_init()
-    S = workload_shells(lib)
+    lib.simint_b200_set_ordering(GAMESS)
+    shells, S = workload_shells(lib)
     t0 = time.time()
     B = sb.Basis(S, TOL, MAX_AM, lib)
     nfull = sum(B.class_full(k) for k in range(len(B.classes())))
@@ -286,7 +337,6 @@ def run_b200(args):
             dist.barrier()
         torch.cuda.synchronize()
         ms = []
-        torch.cuda.nvtx.range_push("timed_" + ("mixed" if prec == sb.MIXED else "fp64"))
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
                 flush.zero_()
@@ -297,7 +347,6 @@ def run_b200(args):
                 e1.record(stream)
                 ms.append((e0, e1))
             torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -314,87 +363,13 @@ def run_b200(args):
     lib.simint_b200_set_precision(sb.FP64, 0.0)
     ct64 = B.class_times(sb.FP64, out.data_ptr(), cap, stream.cuda_stream)
     full = B.output_size <= cap
-    out64 = out.clone() if full else None
+    host64 = out[:B.output_size].cpu().numpy() if (full and rank == 0) else None
     lib.simint_b200_set_precision(sb.MIXED, gate)
     ctmx = B.class_times(sb.MIXED, out.data_ptr(), cap, stream.cuda_stream)
     lib.simint_b200_set_precision(sb.FP64, 0.0)
     torch.cuda.synchronize()
-    # deviation of the mixed path from the FP64 path, per class (full-layout
-    # output only); relative error over elements above 1e-10 of the class max
-    errs = {}
-    if full:
-        for k, c in enumerate(classes):
-            a, n = c["offset"], c["nquart"] * c["nout"]
-            if n == 0:
-                continue
-            d = (out[a:a + n] - out64[a:a + n]).abs()
-            ref = out64[a:a + n].abs()
-            big = ref > 1e-10 * float(ref.max())
-            errs[k] = (float(d.max()), float((d[big] / ref[big]).max()) if bool(big.any()) else 0.0)
-        del out64
-    # Fock digestion of the (mixed) sweep output: Coulomb and exchange
-    # matrices of a seeded symmetric density (simint_b200_basis_jk)
-    jk = None
-    if full:
-        nbf = B.nbf
-        g = torch.Generator(device="cpu").manual_seed(SEED)
-        Dm = torch.rand((nbf, nbf), generator=g, dtype=torch.float64) - 0.5
-        Dm = (0.5 * (Dm + Dm.T)).cuda()
-        Jm = torch.empty_like(Dm)
-        Km = torch.empty_like(Dm)
-        B.jk(out.data_ptr(), cap, Dm.data_ptr(), Jm.data_ptr(), Km.data_ptr(), stream.cuda_stream)
-        torch.cuda.synchronize()
-        jms = []
-        for _ in range(3):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            B.jk(out.data_ptr(), cap, Dm.data_ptr(), Jm.data_ptr(), Km.data_ptr(), stream.cuda_stream)
-            e1.record(stream)
-            e1.synchronize()
-            jms.append(e0.elapsed_time(e1))
-        jt = statistics.median(jms)
-        nq = sum(c["nquart"] for c in classes)
-        ob = B.output_size * 8
-        hbm = None
-        mp = os.path.join(ROOT, "MEASURED_PEAKS.json")
-        if os.path.exists(mp):
-            hbm = json.load(open(mp)).get("hbm_gbs")
-        jk = {"ms": jt, "quartets_s": nq / jt * 1e3, "integrals_gb_s": ob / jt / 1e6, "nbf": nbf,
-              "hbm_frac": (ob / jt / 1e6) / hbm if hbm else None,
-              "note": "J and K of a seeded symmetric density from the sweep sample's integrals "
-                      "(reads every integral once from HBM; fraction of the measured copy bandwidth)"}
-        del Dm, Jm, Km
-    # one-electron matrices of the same basis (simint_b200_oei_matrix):
-    # overlap, kinetic energy and the nuclear attraction of the workload's
-    # pseudo-atoms (distinct shell centres) as point charges Z = 6
-    oei = None
-    if full:
-        atoms = np.unique(np.array([[S.arr[i].x, S.arr[i].y, S.arr[i].z] for i in range(S.n)]), axis=0)
-        cen = np.concatenate([atoms, np.full((len(atoms), 1), 6.0)], axis=1)
-        nbf = B.nbf
-        M = torch.empty((nbf, nbf), dtype=torch.float64, device="cuda")
-        npp = sum(S.arr[i].nprim * S.arr[j].nprim for i in range(S.n) for j in range(i + 1))
-        oei = {"nbf": nbf, "ncentre": len(atoms), "shell_pairs": S.n * (S.n + 1) // 2,
-               "primitive_pairs": npp,
-               "note": "overlap, kinetic and nuclear-attraction matrices of the basis (every unique "
-                       "shell pair, both triangles written); potential over the pseudo-atoms, Z = 6"}
-        for kind, name in ((sb.OEI_OVERLAP, "overlap"), (sb.OEI_KINETIC, "kinetic"),
-                           (sb.OEI_POTENTIAL, "potential")):
-            sb.oei_matrix(kind, S, cen, M.data_ptr(), stream.cuda_stream, lib)
-            torch.cuda.synchronize()
-            t = []
-            for _ in range(3):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                sb.oei_matrix(kind, S, cen, M.data_ptr(), stream.cuda_stream, lib)
-                e1.record(stream)
-                e1.synchronize()
-                t.append(e0.elapsed_time(e1))
-            oei[name + "_ms"] = statistics.median(t)
-        oei["potential_items_s"] = npp * len(atoms) / oei["potential_ms"] * 1e3
-        del M
+    hostmx = out[:B.output_size].cpu().numpy() if (full and rank == 0) else None
+
     total_npq = npq
     if dist:
         from simint_b200.shard import reduce_count_sum
@@ -402,19 +377,6 @@ def run_b200(args):
     value = total_npq / (msmx / 1e3)
     value64 = total_npq / (ms64 / 1e3)
 
-    per_class = []
-    for k, c in enumerate(classes):
-        fl = flops_of_class(c["am"], c["nprimq"], c["nquart"])
-        per_class.append({"am": "".join("spdfg"[x] for x in c["am"]), "quartets": c["nquart"],
-                          "primq": c["nprimq"], "ms_fp64": round(ct64[k], 4), "ms_mixed": round(ctmx[k], 4),
-                          "primq_s_fp64": c["nprimq"] / max(ct64[k], 1e-9) * 1e3,
-                          "primq_s_mixed": c["nprimq"] / max(ctmx[k], 1e-9) * 1e3,
-                          "fp64_tflops": fl / max(ct64[k], 1e-9) / 1e9,
-                          "checksum_fp64": float(sums64[k, 0]), "checksum_mixed": float(sumsmx[k, 0]),
-                          "abssum_fp64": float(sums64[k, 1]),
-                          "variant_fp64": B.variant(c["am"], sb.FP64), "variant_mixed": B.variant(c["am"], sb.MIXED),
-                          "mixed_max_abs_err": errs.get(k, (None, None))[0],
-                          "mixed_max_rel_err": errs.get(k, (None, None))[1]})
     dom = max(range(len(classes)), key=lambda k: ctmx[k])
     dc = classes[dom]
     dom_fl = flops_of_class(dc["am"], dc["nprimq"], dc["nquart"])
@@ -425,14 +387,14 @@ def run_b200(args):
     traffic = None
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
-        ent = json.load(open(prof)).get("".join("spdfg"[x] for x in dc["am"]))
+        ent = json.load(open(prof)).get(amname(dc["am"]))
         if ent:
             traffic = ent["dram_bytes_per_quartet"] * dc["nquart"]
 
-    # e2e through the reference-facing C ABI, host buffers
-    e2e = None
-    cpu = None
+    e2e = cpu = check = None
+    per_check = [{} for _ in classes]
     if rank == 0:
+        # e2e through the reference-facing C ABI, host buffers
         rows = e2e_rows(sb, lib, S, B, max(1, args.e2e_stride // args.stride))
         lib.simint_b200_set_precision(sb.MIXED, gate)
         npq_e2e = sum(sb.count_primq(P, Q, TOL, lib) for _, P, Q in rows)
@@ -456,12 +418,51 @@ def run_b200(args):
         e2e = {"value": npq_e2e / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "calls_per_step": len(rows), "primq_per_step": int(npq_e2e)}
-        if not args.no_cpu:
+        del bufs, rows
+        # the reference's generated CPU library on the host cores, same rows
+        reflib, refsweep, R = load_reference() if not (args.no_cpu and args.no_check) else (None, None, "")
+        if reflib is not None:
             threads = os.cpu_count() or 1
-            rate, t, n, nr = cpu_bench(rows, args.cpu_seconds, threads)
-            cpu = {"value": rate, "unit": "primitive quartets/s", "cores": threads, "kind": "port",
-                   "sample": "%d of the e2e simint_compute_eri rows (%.3g primitive quartets, %.1f s)"
-                             % (nr, n, t)}
+            RS = refsweep.RefSweep(R, shells, TOL, MAX_AM, stride=args.stride, offset=0,
+                                   threads=threads)
+            if not args.no_cpu:
+                rate, t, n, _ = reference_rate(RS, 1, args.cpu_passes, threads)
+                cpu = {"value": rate, "unit": "primitive quartets/s", "cores": threads,
+                       "kind": "reference",
+                       "sample": "the same %d sampled rows (%.3g primitive quartets, %.2f s per pass, "
+                                 "%d passes), reference %s build" % (len(RS.bh), n, t, args.cpu_passes,
+                                                                      REF_VARIANT)}
+            if not args.no_check and host64 is not None:
+                per_check = check_against_reference(B, classes, {"fp64": host64, "mixed": hostmx},
+                                                     RS, refsweep, S.n, threads)
+                agg = {}
+                for name in ("fp64", "mixed"):
+                    vals = [e[name] for e in per_check if name in e]
+                    agg[name] = {"max_abs": max((v[0] for v in vals), default=None),
+                                 "max_rel": max((v[1] for v in vals), default=None),
+                                 "quartets": sum(v[2] for v in vals),
+                                 "bar_failures": sum(v[3] for v in vals)}
+                check = dict(agg, reference=REF_VARIANT,
+                             bar="abs <= 1e-13 or rel <= 1e-11 (fp64); mixed: max abs <= gate",
+                             gate=gate)
+    del host64, hostmx
+
+    per_class = []
+    for k, c in enumerate(classes):
+        fl = flops_of_class(c["am"], c["nprimq"], c["nquart"])
+        ent = {"am": amname(c["am"]), "quartets": c["nquart"], "primq": c["nprimq"],
+               "ms_fp64": round(ct64[k], 4), "ms_mixed": round(ctmx[k], 4),
+               "primq_s_fp64": c["nprimq"] / max(ct64[k], 1e-9) * 1e3,
+               "primq_s_mixed": c["nprimq"] / max(ctmx[k], 1e-9) * 1e3,
+               "fp64_tflops": fl / max(ct64[k], 1e-9) / 1e9,
+               "checksum_fp64": float(sums64[k, 0]), "checksum_mixed": float(sumsmx[k, 0]),
+               "abssum_fp64": float(sums64[k, 1]),
+               "variant_fp64": B.variant(c["am"], sb.FP64), "variant_mixed": B.variant(c["am"], sb.MIXED)}
+        for name, v in per_check[k].items():
+            ent[name + "_vs_ref"] = {"max_abs": v[0], "max_rel": v[1], "quartets": v[2],
+                                     "bar_failures": v[3]}
+        per_class.append(ent)
+    top = sorted(per_class, key=lambda e: -e["ms_mixed"])[:3]
 
     if rank == 0:
         launches = nlmx // 2 * args.steps      # ERI kernels (checksum kernels excluded)
@@ -469,28 +470,29 @@ def run_b200(args):
             "metric": METRIC,
             "value": value, "unit": "primitive quartets/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": msmx, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the error-estimate gate)",
+            "vs_baseline": None, "dtype": "f64+f32 (FP32 VRR behind the per-integral error gate)",
             "data": "synthetic (seeded cfg2 shells, PCG64 seed 2024)",
             "config": dict(workload_config(args, world), **{
-                       "path": "mixed-precision batched sweep (value); FP64 sweep in fp64",
                        "quartets_per_step": int(sum(c["nquart"] for c in classes)),
                        "primq_per_step": int(total_npq), "full_sweep_quartets": int(nfull),
                        "gate": gate, "l2": "256 MB flush before every timed step",
                        "setup_s": round(setup_s, 1), "autotune_s": round(tune_s, 1)}),
             "fp64": {"value": value64, "ms_per_step": ms64},
-            "mixed_vs_fp64": {"max_abs_err": max((e[0] for e in errs.values()), default=None),
-                              "max_rel_err": max((e[1] for e in errs.values()), default=None),
-                              "bar_abs": 1e-10, "classes_checked": len(errs)},
-            "roofline": {"bound": "fp64", "kernel": "class " + "".join("spdfg"[x] for x in dc["am"]),
+            "vs_reference_values": check,
+            "roofline": {"bound": "fp64", "kernel": "class " + amname(dc["am"]),
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 > 0 else None, "traffic": traffic,
-                         "peak_source": "measured FP64 FMA-chain probe (simint_b200_fma_peak), of measured",
-                         "flop_model": "reference generator op counts per unique class (simint_b200.perfmodel)",
-                         "fp32_peak": peak32},
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "fock_jk": jk, "one_electron": oei,
-            "clocks": clkmx, "clocks_fp64": clk64, "per_class": per_class,
+                         "peak_source": "measured FP64 FMA-chain probe, of measured"},
+            "top_classes": [{"am": e["am"], "ms": e["ms_mixed"], "tflops": e["fp64_tflops"]} for e in top],
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clkmx,
         }
-        print(json.dumps(res))
+        if args.detail:
+            d = os.path.dirname(os.path.abspath(args.detail))
+            os.makedirs(d, exist_ok=True)
+            with open(args.detail, "w") as f:
+                json.dump(dict(res, per_class=per_class, clocks_fp64=clk64, fp32_peak=peak32), f)
+        print(compact(res))
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -117,6 +117,10 @@ int simint_b200_basis_class_info(simint_b200_basis const * b, int k, int am[4],
  * shells[0..3] = indices into the shell array given to basis_create. */
 int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, int shells[4]);
 
+/* The same for every quartet of class k at once: shells[4q .. 4q+3] for
+ * q < the class's quartet count (host array of 4 ints per quartet). */
+int simint_b200_basis_class_quartets(simint_b200_basis const * b, int k, int * shells);
+
 /* Per-class checksums of the last compute: sums[2k] = sum of values,
  * sums[2k+1] = sum of absolute values.  Waits for the stream. */
 int simint_b200_basis_checksums(simint_b200_basis * b, double * sums);

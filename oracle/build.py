@@ -15,11 +15,12 @@ TEST INFRASTRUCTURE ONLY.
   with small glue files from oracle/ (ref_shim*.c*) and two configuration
   headers that the reference's CMake would otherwise generate
   (ostei_config.h, vectorization.h: 8-wide layout for the pair code, scalar
-  layout for the Boys glue).  The reference's per-class ERI kernels exist only
-  as output of its code generator (create.py + CMake), so they are not built.
+  layout for the Boys glue).  The reference's per-class ERI kernels (output of
+  its code generator) are built separately by oracle/build_reflib.py.
 
 Run `python oracle/build.py` (or __graft_entry__.build()).  The reference tree
-is read from $SIMINT_REFERENCE (default /root/reference) and only when present.
+is given as an argument or by $SIMINT_REFERENCE (no default), and is used only
+when present.
 """
 
 import os
@@ -29,7 +30,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 GEN = os.path.join(REPO, "simint-generator_b200", "csrc", "gen")
-REF = os.environ.get("SIMINT_REFERENCE", "/root/reference")
+REF = os.environ.get("SIMINT_REFERENCE")
 
 
 def _run(cmd):
@@ -109,9 +110,12 @@ def _write(path, text):
             f.write(text)
 
 
-def build_ref(force=False):
+def build_ref(force=False, ref=None):
     """Compile the reference's hand-written pieces into oracle/_ref/."""
-    skel = os.path.join(REF, "skel")
+    ref = ref or REF
+    if not ref:
+        return None
+    skel = os.path.join(ref, "skel")
     if not os.path.isdir(skel):
         return None
     _ensure_boys()
@@ -161,4 +165,4 @@ def build_ref(force=False):
 
 if __name__ == "__main__":
     print(build_oracle(force=True))
-    print(build_ref(force=True))
+    print(build_ref(force=True, ref=sys.argv[1] if len(sys.argv) > 1 else None))

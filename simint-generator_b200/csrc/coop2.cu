@@ -474,6 +474,9 @@ __global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT == 128 ? 4 : 2)) k_coop
         {
             c.gL = L;
             c.gamp = hrr_amp(c, min(am[0], am[1]), min(am[2], am[3]));
+            // the gate bounds the error of one integral: each of the shell
+            // quartet's primitive quartets may take gate / (their number)
+            c.gate = a.gate / (double)max(1, (c.bi1 - c.bi0) * (c.kj1 - c.kj0));
         }
         for(int k = tid; k < p.acc_size; k += NT)
             acc[k] = 0.0;

@@ -521,6 +521,27 @@ extern "C" int simint_b200_basis_quartet(simint_b200_basis const * b, int k, lon
     return 0;
 }
 
+extern "C" int simint_b200_basis_class_quartets(simint_b200_basis const * b, int k, int * sh)
+{
+    if(!b || !sh || k < 0 || k >= (int)b->qcs.size())
+        return SIMINT_B200_ERR_ARG;
+    const QClass & q = b->qcs[k];
+    const PairClass & X = b->pcs[q.bx];
+    const PairClass & Y = b->pcs[q.ky];
+    long long t = 0;
+    for(size_t r = 0; r + 1 < q.prefix.size(); r++)
+    {
+        const int ip = q.border[r];
+        for(long long i = 0; i < q.prefix[r + 1] - q.prefix[r]; i++, t++)
+        {
+            const int iq = Y.order[(size_t)i];
+            sh[4 * t] = X.sa[ip]; sh[4 * t + 1] = X.sb[ip];
+            sh[4 * t + 2] = Y.sa[iq]; sh[4 * t + 3] = Y.sb[iq];
+        }
+    }
+    return 0;
+}
+
 // Issue the launches of class k (ERI chunks + checksums) on `stream`.
 static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout, long long cap,
                        cudaStream_t stream)

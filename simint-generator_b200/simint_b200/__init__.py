@@ -287,6 +287,15 @@ class Basis:
             raise IndexError((k, q))
         return tuple(sh)
 
+    def class_quartets(self, k, nquart):
+        """(nquart, 4) int array: the shells of every quartet of class k."""
+        sh = np.zeros((max(nquart, 1), 4), dtype=np.int32)
+        self.lib.simint_b200_basis_class_quartets.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        r = self.lib.simint_b200_basis_class_quartets(self.h, k, C.c_void_p(sh.ctypes.data))
+        if r != 0:
+            raise IndexError(k)
+        return sh[:nquart]
+
     def compute(self, prec, dev_ptr, ndoubles, stream=0):
         r = self.lib.simint_b200_basis_compute(self.h, prec, C.c_void_p(dev_ptr), ndoubles,
                                                C.c_void_p(stream))

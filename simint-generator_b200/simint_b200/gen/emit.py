@@ -93,9 +93,21 @@ def emit_class(am, prec="f64", warp=False):
     w("// ---- class (%s) : L=%d, %d top quartets, %d VRR elements, %d HRR steps"
       % (name, L, ntop, len(vrr), sum(1 for _, r in hrr if r is not None)))
     fn = "ostei_%s_%s%s" % (name, prec, "_w" if warp else "")
+    # a class without recursion (L = 0) has no VRR to run in FP32
+    mixed = prec == "mixed" and L > 0
     w("template<bool MIXED_GATE>")
-    w("__device__ __forceinline__ void %s(const QuartetCtx& c, double* __restrict__ out)" % fn)
+    w("__device__ __forceinline__ void %s(const QuartetCtx& c0, double* __restrict__ out)" % fn)
     w("{")
+    w("    QuartetCtx c = c0;")
+    if mixed:
+        # the gate bounds the error of one integral: each of the shell
+        # quartet's primitive quartets may take gate / (their number)
+        w("    if(MIXED_GATE)")
+        w("    {")
+        w("        c.gL = %d;" % L)
+        w("        c.gamp = hrr_amp(c, %d, %d);" % (min(am[0], am[1]), min(am[2], am[3])))
+        w("        c.gate = c0.gate / (double)max(1, (c.bi1 - c.bi0) * (c.kj1 - c.kj0));")
+        w("    }")
     for k in range(ntop):
         w("    double acc%d = 0.0;" % k)
     if warp:
@@ -194,7 +206,7 @@ def emit_class(am, prec="f64", warp=False):
                 lines.append("            acc%d += (double)%s;" % (k, v))
         return lines
 
-    if prec == "f64":
+    if not mixed:
         o.extend(emit_vrr("double", "fma", ""))
     else:
         w("            if(MIXED_GATE && s.lowprec)")

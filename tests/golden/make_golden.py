@@ -15,6 +15,10 @@ shells normalised with the reference's simint_normalize_shells.
 Outputs (numpy .npz, a few hundred kB in total):
   valeev_deriv0.npz  every class up to (dd|dd), Psi4 order
   valeev_deriv1.npz  every class up to (pp|pp) and a set of d classes
+  valeev_fg.npz      f and g classes (deriv 0) with 1-6 primitives, exponents
+                     in [0.05, 5e4] (the benchmark configurations' range) and
+                     centres in a 6 bohr box; ValeevRef in Psi4 order
+  valeev_fg_d1.npz   f classes, deriv 1, the same ranges
   boys_ref.npz       reference boys_F_split values and grid rows
   pairs_ref.npz      reference multi-shell-pair arrays (no screening and
                      fast Schwarz), for bit-exact checks of our pair code
@@ -22,7 +26,7 @@ Outputs (numpy .npz, a few hundred kB in total):
                      energy, nuclear attraction; skel/simint/osoei) for every
                      (la|lb) up to (g|g)
 
-`--oei-only` regenerates oei_ref.npz alone.
+`--oei-only` regenerates oei_ref.npz alone; `--fg-only` the f/g files alone.
 """
 
 import ctypes as C
@@ -71,12 +75,12 @@ def valeev(ref, S, grp, deriv):
     return out
 
 
-def make_valeev(ref, deriv, classes, nsh, nprim, seed):
+def make_valeev(ref, deriv, classes, nsh, nprim, seed, alpha=(0.15, 12.0), box=2.5):
     rng = np.random.default_rng(seed)
     data = {}
     for am in classes:
         ams = sum(([am[k]] * nsh[k] for k in range(4)), [])
-        shells = random_shells(rng, ams, nprim_range=nprim, alpha=(0.15, 12.0), box=2.5)
+        shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box)
         S = normalized(ref, shells)
         # store the normalised coefficients so users skip normalisation
         norm = [(s[0], s[1], s[2], S.coefs(k)) for k, s in enumerate(shells)]
@@ -170,6 +174,9 @@ def main():
     ref = load_ref()
     if ref is None:
         raise SystemExit("oracle/_ref/libsimint_ref.so missing: run python oracle/build.py here")
+    if "--fg-only" in sys.argv:
+        make_fg(ref)
+        return
     np.savez_compressed(os.path.join(HERE, "oei_ref.npz"), **make_oei(ref))
     if "--oei-only" in sys.argv:
         return
@@ -184,6 +191,24 @@ def main():
                         **make_valeev(ref, 1, d1, (1, 1, 2, 1), (1, 2), 12))
     np.savez_compressed(os.path.join(HERE, "boys_ref.npz"), **make_boys(ref))
     np.savez_compressed(os.path.join(HERE, "pairs_ref.npz"), **make_pairs(ref))
+    make_fg(ref)
+
+
+# f and g classes of the benchmark workloads (the dominant (fd|fp), (fd|dp),
+# (ff|fd) of the l <= 3 sweep, g classes of the l <= 4 sweep)
+FG_D0 = [(3, 0, 0, 0), (3, 0, 3, 0), (3, 1, 3, 0), (3, 2, 1, 1), (3, 2, 2, 1), (3, 2, 3, 1),
+         (3, 3, 2, 2), (3, 3, 3, 2), (3, 3, 3, 3), (2, 2, 3, 3), (4, 0, 0, 0), (4, 1, 2, 0),
+         (4, 0, 4, 0), (4, 2, 3, 1), (4, 4, 0, 0), (4, 3, 2, 2), (4, 4, 2, 1)]
+FG_D1 = [(3, 0, 0, 0), (3, 1, 1, 0), (3, 2, 1, 1), (3, 1, 2, 2), (2, 2, 3, 0)]
+
+
+def make_fg(ref):
+    np.savez_compressed(os.path.join(HERE, "valeev_fg.npz"),
+                        **make_valeev(ref, 0, FG_D0, (1, 1, 1, 2), (1, 4), 13,
+                                      alpha=(0.05, 5e4), box=6.0))
+    np.savez_compressed(os.path.join(HERE, "valeev_fg_d1.npz"),
+                        **make_valeev(ref, 1, FG_D1, (1, 1, 1, 1), (1, 3), 14,
+                                      alpha=(0.05, 5e4), box=6.0))
 
 
 if __name__ == "__main__":

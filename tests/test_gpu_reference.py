@@ -1,0 +1,340 @@
+"""GPU: libsimint_b200.so against the reference's own generated CPU library
+(create.py output built by oracle/build_reflib.py) on the shells of the
+benchmark configurations.
+
+Both libraries receive identical calls from one C driver (oracle/refdrv.c:
+compiled into every reference build, and against include/ as
+oracle/_ref/librefdrv_b200.so for ours): each library builds its own shells,
+normalisation and shell pairs from the same inputs and runs
+simint_compute_eri(_deriv) over the same rows (one bra pair against a list
+of kets, the way the reference's test_eri and benchmark_eri call it).
+
+Bar per element (FP64): abs <= 1e-13, or |ref| > 1e-15 and rel <= 1e-11.
+A quartet outside the bar passes only when it is ill-conditioned in double
+precision and we are no less accurate than the reference on it: our values
+are at most 2x as far from a long-double evaluation (oracle/liboracle_ld.so)
+as the reference's values are (+1e-14).  The reference's own two builds
+(default and all-inline generation) disagree beyond the bar on about 1 in
+1e5 quartets of the l <= 3 workload (exponents 0.05-5e4 on distant centres
+make the recurrences cancel), so no implementation can hold the bar there.
+
+  cfg1  64 s/p shells, every unique shell quartet (2 164 240), GAMESS order,
+        screen_tol 0 (the all-inline GAMESS build: true GAMESS order)
+  cfg2  a seeded row sample of the l <= 3 Schwarz-screened sweep at 1e-14
+        (GAMESS order), primitive screening as the reference does it
+  cfg5  every 8th shell of the l <= 4 configuration, screened at 1e-12, a row
+        sample (Psi4 order, default generation)
+  cfg4  deriv 1, a row sample of the l <= 2 configuration (Psi4 order; the
+        reference's GAMESS deriv1 indexes through the Psi4 table), and
+        central finite differences of our FP64 ERIs (h = 1e-4 bohr)
+  ValeevRef f/g fixtures (tests/golden/valeev_fg*.npz): our GPU path against
+        the reference's long-double oracle directly, at the configurations'
+        exponent ranges.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import simint_b200 as sb
+import reflib
+import refsweep
+from simint_b200.workloads import config_shells
+from oracle import load_oracle, load_oracle_ld
+from _util import parity_bad, quartets_unexplained, RowLD, NC
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DRV = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "librefdrv_b200.so")
+
+
+def need(variant):
+    if not reflib.available(variant):
+        pytest.skip("reference library %s not built (oracle/build_reflib.py)" % variant)
+    return reflib.load(variant)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    L = sb.load()
+    L.simint_init()
+    return L
+
+
+@pytest.fixture(scope="module")
+def drv(lib):
+    if not os.path.exists(DRV):
+        import build_chost
+        build_chost.build_driver()
+    return reflib.RefLib(DRV)
+
+
+def cfg1_rows(shells):
+    """Every unique quartet (pair p >= pair r, pairs i >= j): per bra pair p,
+    one row per ket class (am_k, am_l), the class's pairs in pair order
+    clipped at p."""
+    n = len(shells)
+    pairs = [(i, j) for i in range(n) for j in range(i + 1)]
+    cls = {}
+    for r, (k, l) in enumerate(pairs):
+        cls.setdefault((shells[k][0], shells[l][0]), []).append(r)
+    keys = sorted(cls)
+    rows = []
+    for p, (i, j) in enumerate(pairs):
+        for c in keys:
+            idx = np.asarray(cls[c])
+            cnt = int(np.searchsorted(idx, p, side="right"))
+            if cnt:
+                rows.append((p, keys.index(c), cnt))
+    return pairs, keys, cls, rows
+
+
+def run_rows(D, shells, pairs, keys, cls, rows, ordering_lib=None, threads=None):
+    D.set_shells(shells)
+    kh = D.pairsets_multi([[pairs[r] for r in cls[c]] for c in keys], 0, threads)
+    bras = sorted({p for p, _, _ in rows})
+    bh = dict(zip(bras, D.pairsets_single([pairs[p] for p in bras], 0, threads)))
+    b = np.array([bh[p] for p, _, _ in rows], np.int32)
+    k = np.array([kh[c] for _, c, _ in rows], np.int32)
+    kc = np.array([cnt for _, _, cnt in rows], np.int32)
+    nout = np.array([NC(shells[pairs[p][0]][0]) * NC(shells[pairs[p][1]][0]) * NC(keys[c][0])
+                     * NC(keys[c][1]) for p, c, _ in rows], np.int64)
+    sizes = kc * nout
+    off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    out = np.zeros(int(sizes.sum()))
+    _, ret, _ = D.rows(b, k, kc, 0, 0.0, threads, out=out, off=off, count=False)
+    D.free_pairsets()
+    return ret, out
+
+
+def test_cfg1_all_quartets_gamess(lib, drv):
+    R = need("gamess_l3")
+    shells = config_shells("cfg1")
+    pairs, keys, cls, rows = cfg1_rows(shells)
+    nq = sum(cnt for _, _, cnt in rows)
+    assert nq == 2164240
+    lib.simint_b200_set_ordering(sb.GAMESS)
+    try:
+        rr, ref = run_rows(R, shells, pairs, keys, cls, rows)
+        rg, calc = run_rows(drv, shells, pairs, keys, cls, rows, threads=1)
+    finally:
+        lib.simint_b200_set_ordering(sb.PSI4)
+    assert (rr == rg).all()
+    ld = RowLD(load_oracle(), load_oracle_ld(), shells, ordering=sb.GAMESS)
+    # quartets row by row (nout differs between rows): judge the rows
+    # holding elements outside the bar
+    pos = 0
+    nover = 0
+    for p, c, cnt in rows:
+        nout = NC(shells[pairs[p][0]][0]) * NC(shells[pairs[p][1]][0]) * NC(keys[c][0]) * NC(keys[c][1])
+        n = cnt * nout
+        bad, _ = parity_bad(calc[pos:pos + n], ref[pos:pos + n])
+        if len(bad):
+            kets = [pairs[r] for r in cls[keys[c]]]
+            ub, no = quartets_unexplained(calc[pos:pos + n], ref[pos:pos + n],
+                                          lambda q: ld(pairs[p], kets[q]), nout)
+            assert not ub, (p, c, ub[:3])
+            nover += no
+        pos += n
+    assert nover <= 10, nover
+
+
+def sweep_case(lib, drv, variant, shells, tol, max_am, stride, ordering, deriv=0):
+    R = need(variant)
+    lib.simint_b200_set_ordering(ordering)
+    try:
+        S = refsweep.RefSweep(R, shells, tol, max_am, stride=stride, offset=stride // 3)
+        ref, off = S.outputs(deriv=deriv)
+        bh, kh, kc = S.mirror(drv, shells)
+        calc = np.zeros_like(ref)
+        _, ret, _ = drv.rows(bh, kh, kc, deriv, tol, 1, out=calc, off=off, count=False)
+    finally:
+        lib.simint_b200_set_ordering(sb.PSI4)
+        drv.free_pairsets()
+    return S, ref, calc
+
+
+def check_rows(S, shells, calc, ref, tol, deriv, ordering):
+    """Per class: the bar, with ill-conditioned quartets judged against the
+    long-double evaluation.  Returns (quartets, outside the bar)."""
+    ld = RowLD(load_oracle(), load_oracle_ld(), shells, screen=1 if tol > 0 else 0, tol=tol,
+               deriv=deriv, ordering=ordering)
+    off, _ = S.layout(deriv)
+    nq = 0
+    nover = 0
+    for k, q in enumerate(S.qcs):
+        rows = np.nonzero(S.cls == k)[0]
+        if len(rows) == 0:
+            continue
+        nout = int(np.prod([NC(x) for x in q["am"]])) * (12 if deriv else 1)
+        a = off[rows[0]]
+        n = int(S.kc[rows].sum()) * nout
+        cum = np.concatenate([[0], np.cumsum(S.kc[rows])])
+        kets = S.ket_lists[S.ket_index[q["ky"]]]
+
+        def ld_of(qi, rows=rows, cum=cum, kets=kets):
+            rl = int(np.searchsorted(cum, qi, side="right")) - 1
+            r = rows[rl]
+            return ld(tuple(S.bra_pairs[r]), tuple(kets[qi - cum[rl]]))
+
+        bad, nout_bar = quartets_unexplained(calc[a:a + n], ref[a:a + n], ld_of, nout)
+        assert not bad, (q["am"], bad[:5])
+        nq += n // nout
+        nover += nout_bar
+    return nq, nover
+
+
+def test_cfg2_rows_gamess(lib, drv):
+    shells = config_shells("cfg2")
+    S, ref, calc = sweep_case(lib, drv, "gamess_l3", shells, 1e-14, 3, 997, sb.GAMESS)
+    assert S.nquartets > 50000 and len(set(S.cls)) == len(S.qcs)
+    nq, nover = check_rows(S, shells, calc, ref, 1e-14, 0, sb.GAMESS)
+    assert nover <= 1e-4 * nq, (nover, nq)
+
+
+def test_cfg5_rows_psi4(lib, drv):
+    shells = config_shells("cfg5")[::8]
+    S, ref, calc = sweep_case(lib, drv, "psi4_l4", shells, 1e-12, 4, 211, sb.PSI4)
+    assert max(max(q["am"]) for q in S.qcs) == 4
+    nq, nover = check_rows(S, shells, calc, ref, 1e-12, 0, sb.PSI4)
+    assert nover <= 1e-3 * nq, (nover, nq)
+
+
+def test_cfg4_deriv1_rows_psi4(lib, drv):
+    shells = config_shells("cfg4")
+    S, ref, calc = sweep_case(lib, drv, "psi4_d1_l2", shells, 1e-14, 2, 401, sb.PSI4, deriv=1)
+    assert S.nquartets > 10000
+    nq, nover = check_rows(S, shells, calc, ref, 1e-14, 1, sb.PSI4)
+    assert nover <= 1e-3 * nq, (nover, nq)
+
+
+def test_cfg4_deriv1_finite_differences(lib, drv):
+    """Analytic gradients of our FP64 path against central differences of
+    our FP64 ERIs: each centre of a quartet moved by +-h along x, y, z
+    (h = 1e-4 bohr).  Agreement to 1e-7 of the gradient scale (the O(h^2)
+    truncation) plus 1e-10 absolute (rounding / h)."""
+    shells = config_shells("cfg4")
+    rng = np.random.default_rng(5)
+    h = 1e-4
+    lib.simint_b200_set_ordering(sb.PSI4)
+    for trial in range(6):
+        q = [int(x) for x in rng.choice(len(shells), 4, replace=False)]
+        base = [shells[k] for k in q]
+        drv.set_shells(base)
+        P = drv.pairset([(0, 1)])
+        Q = drv.pairset([(2, 3)])
+        nout = int(np.prod([NC(s[0]) for s in base]))
+        g = np.zeros(nout * 12)
+        drv.rows([P], [Q], [0], 1, 0.0, 1, out=g, off=[0], count=False)
+        drv.free_pairsets()
+        g = g.reshape(nout, 12)
+        fd = np.zeros_like(g)
+        for ctr in range(4):
+            for x in range(3):
+                vals = []
+                for sgn in (1, -1):
+                    moved = list(base)
+                    am, xyz, al, co = moved[ctr]
+                    c = list(xyz)
+                    c[x] += sgn * h
+                    moved[ctr] = (am, tuple(c), al, co)
+                    drv.set_shells(moved)
+                    P = drv.pairset([(0, 1)])
+                    Q = drv.pairset([(2, 3)])
+                    v = np.zeros(nout)
+                    drv.rows([P], [Q], [0], 0, 0.0, 1, out=v, off=[0], count=False)
+                    drv.free_pairsets()
+                    vals.append(v)
+                fd[:, ctr * 3 + x] = (vals[0] - vals[1]) / (2 * h)
+        scale = max(float(np.abs(g).max()), 1e-12)
+        err = np.abs(fd - g)
+        assert (err <= 1e-7 * scale + 1e-10).all(), (q, float(err.max()), scale)
+
+
+def _fixture_cases(path):
+    d = np.load(path)
+    names = sorted({k.split("/")[0] for k in d.keys()})
+    for name in names:
+        am, xyz, npr = d[name + "/am"], d[name + "/xyz"], d[name + "/nprim"]
+        al, co = d[name + "/alpha"], d[name + "/coef"]
+        off = np.concatenate([[0], np.cumsum(npr)])
+        shells = [(int(am[k]), tuple(xyz[k]), al[off[k]:off[k + 1]], co[off[k]:off[k + 1]])
+                  for k in range(len(am))]
+        nsh = d[name + "/nsh"]
+        idx = np.concatenate([[0], np.cumsum(nsh)])
+        grp = [list(range(idx[k], idx[k + 1])) for k in range(4)]
+        yield name, shells, grp, d[name + "/values"].ravel()
+
+
+@pytest.mark.parametrize("fname,deriv", [("valeev_fg.npz", 0), ("valeev_fg_d1.npz", 1)])
+def test_gpu_matches_valeev_fg(lib, drv, fname, deriv):
+    """Our GPU path against ValeevRef (the reference's long-double oracle)
+    on f and g classes; the reference's own acceptance rule and the FP64
+    bar of the configurations."""
+    path = os.path.join(HERE, "golden", fname)
+    lib.simint_b200_set_ordering(sb.PSI4)
+    for name, shells, grp, ref in _fixture_cases(path):
+        drv.set_shells(shells, normalize=False)
+        bra = [(a, b) for a in grp[0] for b in grp[1]]
+        ket = [(c, d) for c in grp[2] for d in grp[3]]
+        kh = drv.pairset(ket)
+        bh = drv.pairsets_single(bra, 0, 1)
+        nout = int(np.prod([NC(shells[g[0]][0]) for g in grp])) * (12 if deriv else 1)
+        out = np.zeros(len(bra) * len(ket) * nout)
+        off = np.arange(len(bra), dtype=np.int64) * len(ket) * nout
+        drv.rows(bh, np.full(len(bh), kh, np.int32), np.zeros(len(bh), np.int32), deriv, 0.0, 1,
+                 out=out, off=off, count=False)
+        drv.free_pairsets()
+        d = np.abs(out - ref)
+        rel = d / np.maximum(np.abs(ref), 1e-300)
+        assert not ((d > 1e-14) & (rel > 1e-8) & (np.abs(ref) > 1e-15)).any(), (name, float(d.max()))
+        bad, dmax = parity_bad(out, ref)
+        assert len(bad) == 0, (name, dmax)
+
+
+def test_sweep_against_reference(lib):
+    """The batched sweep (simint_b200_basis_*, FP64 and mixed) against the
+    reference's values of the same quartets: every 4th shell of cfg2, the
+    whole screened sweep.  FP64 within the bar; mixed within the gate."""
+    torch = pytest.importorskip("torch")
+    R = need("gamess_l3")
+    from simint_b200.capi import ShellSet
+    shells = config_shells("cfg2")[::4]
+    lib.simint_b200_set_ordering(sb.GAMESS)
+    gate = 1e-10
+    try:
+        S = ShellSet(shells)
+        lib.simint_normalize_shells(S.n, S.ptr(0))
+        B = sb.Basis(S, 1e-14, 3, lib)
+        classes = B.classes()
+        n = B.output_size
+        out = torch.empty(n, dtype=torch.float64, device="cuda")
+        B.compute(sb.FP64, out.data_ptr(), n)
+        torch.cuda.synchronize()
+        h64 = out.cpu().numpy()
+        lib.simint_b200_set_precision(sb.MIXED, gate)
+        B.compute(sb.MIXED, out.data_ptr(), n)
+        torch.cuda.synchronize()
+        hmx = out.cpu().numpy()
+    finally:
+        lib.simint_b200_set_precision(sb.FP64, 0.0)
+        lib.simint_b200_set_ordering(sb.PSI4)
+    RS = refsweep.RefSweep(R, shells, 1e-14, 3)
+    ref_out, _ = RS.outputs()
+    byam = {tuple(q["am"]): k for k, q in enumerate(RS.qcs)}
+    ncmp = 0
+    for k, c in enumerate(classes):
+        keys, offs = RS.class_keys(byam[tuple(c["am"])], len(shells))
+        sh4 = B.class_quartets(k, c["nquart"])
+        a, m = c["offset"], c["nquart"] * c["nout"]
+        ma, mr, nc, nbad = refsweep.compare_class(ref_out, keys, offs, h64[a:a + m], sh4, c["nout"],
+                                                  len(shells))
+        assert nbad == 0, (c["am"], ma, mr)
+        assert nc >= 0.99 * c["nquart"], (c["am"], nc, c["nquart"])
+        ncmp += nc
+        ma, mr, nc, nbad = refsweep.compare_class(ref_out, keys, offs, hmx[a:a + m], sh4, c["nout"],
+                                                  len(shells))
+        assert ma <= gate, (c["am"], ma)
+    assert ncmp > 100000
+    B.close()

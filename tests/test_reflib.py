@@ -1,0 +1,196 @@
+"""CPU: the reference's generated library (oracle/_ref, built by
+oracle/build_reflib.py) pinned to the reference's own long-double oracle,
+and our CPU restatement (oracle/ostei_oracle.c) pinned to that library above
+l = 2 and at the configurations' exponent ranges.
+
+* ValeevRef fixtures (tests/golden/valeev_*.npz, made by the reference's
+  skel/test/ValeevRef.cpp) against the generated library: every class of the
+  fixtures meets the reference's own acceptance rule
+  (skel/test/test_eri.cpp:227: failure only when abs > 1e-14 and rel > 1e-8).
+* The all-inline GAMESS build equals the Psi4 build with every d and f
+  shell's Cartesians permuted (generator/Ordering_GAMESS.cpp:8-41).
+* Our oracle against the generated library on random f and g classes with
+  exponents in [0.05, 5e4] and 1-6 primitives: the FP64 bar (abs 1e-13 or
+  rel 1e-11), ill-conditioned quartets judged against the long-double
+  evaluation (_util.quartets_unexplained).
+"""
+import ctypes as C
+import itertools
+
+import numpy as np
+import pytest
+
+import reflib
+from oracle import load_oracle, load_oracle_ld
+from simint_b200.capi import ShellSet
+from simint_b200.workloads import random_shells
+from _util import oracle_pairs, oracle_eri, parity_bad, quartets_unexplained, RowLD, NC
+
+GOLD = __import__("os").path.join(__import__("os").path.dirname(__file__), "golden")
+
+
+def need(variant):
+    if not reflib.available(variant):
+        pytest.skip("reference library %s not built (oracle/build_reflib.py)" % variant)
+    return reflib.load(variant)
+
+
+def fixture_classes(path):
+    d = np.load(path)
+    names = sorted({k.split("/")[0] for k in d.keys()})
+    return d, names
+
+
+def fixture_shells(d, name):
+    am, xyz, npr = d[name + "/am"], d[name + "/xyz"], d[name + "/nprim"]
+    al, co = d[name + "/alpha"], d[name + "/coef"]
+    off = np.concatenate([[0], np.cumsum(npr)])
+    shells = [(int(am[k]), tuple(xyz[k]), al[off[k]:off[k + 1]], co[off[k]:off[k + 1]])
+              for k in range(len(am))]
+    nsh = d[name + "/nsh"]
+    idx = np.concatenate([[0], np.cumsum(nsh)])
+    grp = [list(range(idx[k], idx[k + 1])) for k in range(4)]
+    return shells, grp
+
+
+def ref_rect(R, grp, deriv, tol=0.0, screen=0):
+    """Pair sets of the rectangle grp[0] x grp[1] | grp[2] x grp[3]: one
+    single-pair set per bra pair (as test_eri calls it) and the ket list."""
+    bra = [(a, b) for a in grp[0] for b in grp[1]]
+    ket = [(c, d) for c in grp[2] for d in grp[3]]
+    kh = R.pairset(ket, screen)
+    bh = R.pairsets_single(bra, screen, 1)
+    return bh, kh, len(ket)
+
+
+def run_rect(R, shells, grp, deriv, normalize=False, tol=0.0, screen=0):
+    R.set_shells(shells, normalize=normalize)
+    bh, kh, nket = ref_rect(R, grp, deriv, tol, screen)
+    ams = [shells[g[0]][0] for g in grp]
+    nout = int(np.prod([NC(a) for a in ams])) * (12 if deriv else 1)
+    out = np.zeros(len(bh) * nket * nout)
+    off = np.arange(len(bh), dtype=np.int64) * nket * nout
+    _, ret, _ = R.rows(bh, np.full(len(bh), kh, np.int32), np.zeros(len(bh), np.int32), deriv, tol,
+                       1, out=out, off=off, count=False)
+    R.free_pairsets()
+    return ret, out
+
+
+def test_reflib_matches_valeev_deriv0():
+    R = need("psi4_l4")
+    d, names = fixture_classes(GOLD + "/valeev_deriv0.npz")
+    worst = 0.0
+    for name in names:
+        shells, grp = fixture_shells(d, name)
+        ret, out = run_rect(R, shells, grp, 0)
+        ref = d[name + "/values"].ravel()
+        diff = np.abs(out - ref)
+        rel = diff / np.maximum(np.abs(ref), 1e-300)
+        bad = (diff > 1e-14) & (rel > 1e-8) & (np.abs(ref) > 1e-15)
+        assert not bad.any(), (name, float(diff.max()))
+        worst = max(worst, float(diff.max()))
+    assert worst < 1e-13
+
+
+def test_reflib_matches_valeev_deriv1():
+    R = need("psi4_d1_l2")
+    d, names = fixture_classes(GOLD + "/valeev_deriv1.npz")
+    for name in names:
+        shells, grp = fixture_shells(d, name)
+        if max(s[0] for s in shells) > R.max_am:
+            continue
+        ret, out = run_rect(R, shells, grp, 1)
+        ref = d[name + "/values"].ravel()
+        diff = np.abs(out - ref)
+        rel = diff / np.maximum(np.abs(ref), 1e-300)
+        bad = (diff > 1e-14) & (rel > 1e-8) & (np.abs(ref) > 1e-15)
+        assert not bad.any(), (name, float(diff.max()))
+
+
+def test_reflib_matches_valeev_fg():
+    R = need("psi4_l4")
+    path = GOLD + "/valeev_fg.npz"
+    d, names = fixture_classes(path)
+    for name in names:
+        shells, grp = fixture_shells(d, name)
+        ret, out = run_rect(R, shells, grp, 0)
+        ref = d[name + "/values"].ravel()
+        diff = np.abs(out - ref)
+        rel = diff / np.maximum(np.abs(ref), 1e-300)
+        bad = (diff > 1e-14) & (rel > 1e-8) & (np.abs(ref) > 1e-15)
+        assert not bad.any(), (name, float(diff.max()), float(rel[bad].max()))
+
+
+GAMESS_D = [(2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0), (1, 0, 1), (0, 1, 1)]
+GAMESS_F = [(3, 0, 0), (0, 3, 0), (0, 0, 3), (2, 1, 0), (2, 0, 1), (1, 2, 0), (0, 2, 1),
+            (1, 0, 2), (0, 1, 2), (1, 1, 1)]
+
+
+def psi4_list(l):
+    return [(i, j, l - i - j) for i in range(l, -1, -1) for j in range(l - i, -1, -1)]
+
+
+def gamess_perm(l):
+    """Index of each GAMESS-ordered Cartesian in the Psi4 order."""
+    p = psi4_list(l)
+    g = {2: GAMESS_D, 3: GAMESS_F}.get(l, p)
+    return [p.index(c) for c in g]
+
+
+@pytest.mark.parametrize("am", [(2, 1, 2, 0), (3, 2, 1, 1), (3, 3, 2, 2), (2, 2, 3, 3)])
+def test_gamess_inline_is_psi4_permuted(am):
+    Rg = need("gamess_l3")
+    Rp = need("psi4_l4")
+    rng = np.random.default_rng(7)
+    shells = random_shells(rng, list(am), nprim_range=(1, 3), alpha=(0.1, 50.0), box=3.0)
+    grp = [[0], [1], [2], [3]]
+    _, g = run_rect(Rg, shells, grp, 0, normalize=True)
+    _, p = run_rect(Rp, shells, grp, 0, normalize=True)
+    p = p.reshape([NC(a) for a in am])
+    for ax, l in enumerate(am):
+        p = np.take(p, gamess_perm(l), axis=ax)
+    bad, dmax = parity_bad(g, p.ravel())
+    assert len(bad) == 0, dmax
+
+
+# random f/g classes at the configurations' exponent ranges: our oracle
+# against the generated library
+FG = [(3, 2, 3, 1), (3, 2, 2, 1), (3, 3, 3, 2), (3, 3, 3, 3), (4, 0, 0, 0), (4, 1, 2, 0),
+      (4, 2, 3, 1), (4, 4, 2, 2), (4, 3, 4, 1), (3, 1, 4, 4)]
+
+
+@pytest.mark.parametrize("am", FG)
+def test_oracle_matches_reflib_fg(am):
+    R = need("psi4_l4")
+    orc = load_oracle()
+    rng = np.random.default_rng(sum(a * 10 ** k for k, a in enumerate(am)))
+    ams = [am[0], am[0], am[1], am[2], am[3], am[3]]
+    shells = random_shells(rng, ams, nprim_range=(1, 6), alpha=(0.05, 5e4), box=6.0, natom=3)
+    grp = [[0, 1], [2], [3], [4, 5]]
+    R.set_shells(shells)
+    norm = R.coefs()
+    off = np.concatenate([[0], np.cumsum([len(s[2]) for s in shells])])
+    shells_n = [(s[0], s[1], s[2], norm[off[k]:off[k + 1]]) for k, s in enumerate(shells)]
+    _, ref = run_rect(R, shells_n, grp, 0, normalize=False)
+    S = ShellSet(shells_n)
+    P = oracle_pairs(orc, S, [(a, b) for a in grp[0] for b in grp[1]])
+    Q = oracle_pairs(orc, S, [(c, d) for c in grp[2] for d in grp[3]])
+    # one bra pair at a time, like the reference rows
+    outs = []
+    for a in grp[0]:
+        for b in grp[1]:
+            Pi = oracle_pairs(orc, S, [(a, b)])
+            r, o = oracle_eri(orc, Pi, Q)
+            outs.append(o)
+            orc.oracle_free_pair(C.byref(Pi))
+    calc = np.concatenate(outs)
+    orc.oracle_free_pair(C.byref(P))
+    orc.oracle_free_pair(C.byref(Q))
+    # ill-conditioned quartets (see _util.quartets_unexplained) are judged
+    # against the long-double evaluation
+    ld = RowLD(orc, load_oracle_ld(), shells_n, normalize=False)
+    bras = [(a, b) for a in grp[0] for b in grp[1]]
+    kets = [(c, d) for c in grp[2] for d in grp[3]]
+    bad, nover = quartets_unexplained(calc, ref, lambda q: ld(bras[q // len(kets)], kets[q % len(kets)]),
+                                      int(np.prod([NC(a) for a in (am[0], am[1], am[2], am[3])])))
+    assert not bad, (am, bad[:3])
