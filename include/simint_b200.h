@@ -36,16 +36,19 @@ int simint_b200_set_ordering(int ordering);
 int simint_b200_get_ordering(void);
 
 /* FP64 everywhere, or FP32 VRR for primitive quartets whose estimated FP32
- * error is below `gate` (FP64 Boys, prefactors, contraction and HRR in both
- * modes).  The estimate of one primitive quartet of a class with recursion
- * depth L = la+lb+lc+ld is
+ * error keeps every integral within `gate` (FP64 Boys, prefactors,
+ * contraction and HRR in both modes).  The estimate of one primitive quartet
+ * of a class with recursion depth L = la+lb+lc+ld is
  *     8 (L+1) 2^-24 |prefac| r^L (1 + |AB|)^min(la,lb) (1 + |CD|)^min(lc,ld),
  *     r = (g + sqrt(g^2 + 4h)) / 2,  g = 1 + max|X| + max|Y|,
  *     h = L (1/2p + 1/2q + 1/2(p+q))
  * (X: P-A, P-B, Q-C, Q-D components; Y: the rho/p, rho/q (P-Q) terms), a
  * bound on the absolute error its FP32 VRR adds to any integral of the
- * shell quartet; an integral's error is at most the sum over its primitive
- * quartets.  gate = 0 keeps FP64.  Process-wide. */
+ * shell quartet.  An integral's error is at most the sum over its primitive
+ * quartets, so a primitive quartet runs in FP32 only when its estimate is
+ * below gate / (the shell quartet's primitive quartets): the gate bounds
+ * the error of each integral.  Classes with L = 0 stay in FP64 (no VRR).
+ * gate = 0 keeps FP64.  Process-wide. */
 int simint_b200_set_precision(int mode, double gate);
 int simint_b200_get_precision(void);
 
@@ -122,30 +125,60 @@ int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, i
 int simint_b200_basis_class_quartets(simint_b200_basis const * b, int k, int * shells);
 
 /* Per-class checksums of the last compute: sums[2k] = sum of values,
- * sums[2k+1] = sum of absolute values.  Waits for the stream. */
+ * sums[2k+1] = sum of absolute values.  Waits for the device.  Returns
+ * SIMINT_B200_ERR_TIMEOUT when a bounded work-queue wait of the sweep ran
+ * out (see simint_b200_basis_queue_probe). */
 int simint_b200_basis_checksums(simint_b200_basis * b, double * sums);
 
+/* Primitive quartets of the last compute that ran their VRR in FP32 (mixed
+ * precision), per class: counts[k] for every class k (host array of
+ * simint_b200_basis_nclass entries), counted by every kernel with an FP32
+ * path (register, cooperative and column kernels).  Waits for the
+ * device. */
+int simint_b200_basis_fp32_counts(simint_b200_basis * b, long long * counts);
+
+/* Work queue.  The cooperative and column kernels of a sweep take their
+ * shell quartets from a device work queue, one atomic pull per CTA, in
+ * order of decreasing primitive count (the longest quartets first, the
+ * short ones fill the tail).  A CTA that finds no published task waits --
+ * bounded, about one microsecond per poll -- until more are published or
+ * the queue is closed; a wait that runs out marks the queue and the CTA
+ * returns, so the launch always ends.  In a sweep every task is published
+ * before the launch.
+ *
+ * simint_b200_basis_queue_probe runs class k (FP64, its current kernel,
+ * which must be a queue kernel) with a queue whose first `published` tasks
+ * are available and which is closed (closed != 0) or left open, each wait
+ * limited to about wait_ms milliseconds, writing to dev_out (at least the
+ * class's quartets x nout doubles; quartet q at q*nout).  Returns
+ * `published` when every CTA finished normally, SIMINT_B200_ERR_TIMEOUT when
+ * a wait ran out (an open queue), or another negative code.  The device
+ * stays usable after a timeout. */
+int simint_b200_basis_queue_probe(simint_b200_basis * b, int k, long long published, int closed,
+                                  int wait_ms, double * dev_out, long long dev_out_doubles);
+
 /* Autotuner: for every class of the sweep time each kernel variant (the
- * register kernel where one exists, the cooperative kernel with 256 or 128
- * threads and 1, 2 or 4 primitive quartets per wavefront pass) on the
- * sweep's own tasks and keep
- * the fastest for `prec`.  Choices are process-wide and are written to the
+ * register kernel where one exists, thread- and warp-per-quartet; the
+ * cooperative kernel with 256, 128 or 64 threads and 1, 2, 4 or 8
+ * primitive quartets per wavefront pass; the column kernel with 4 or 8
+ * primitive quartets per batch; in mixed mode each also in FP64) on the
+ * sweep's own tasks and keep the fastest for `prec`.  Choices are process-wide and are written to the
  * JSON file $SIMINT_B200_TUNE_FILE when set (read back by simint_init). */
 int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
                                long long dev_out_doubles, void * stream);
 
 /* The kernel variant chosen for a requested class (0 = untuned default,
  * 1 = register kernel, 20+B / 40+B / 60+B = cooperative kernel with 256 /
- * 128 / 64 threads and batch B = 1, 2, 4, 8). */
+ * 128 / 64 threads and batch B = 1, 2, 4, 8, 81 / 82 = column kernel with
+ * 4 / 8 primitive quartets per batch, deriv 0). */
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first
  * cooperative kernel, 4 = generic kernel, 5 = register kernel run in FP64
  * even in mixed mode, 6 = register kernel with one warp per shell quartet,
- * 7 = the same in FP64 even in mixed mode, and 100 + a cooperative code =
- * that kernel in FP64 even
- * in mixed mode (prec must be SIMINT_B200_PREC_MIXED); 0 restores the
- * default rule).
+ * 7 = the same in FP64 even in mixed mode, and 100 + a cooperative or
+ * column code = that kernel in FP64 even in mixed mode (prec must be
+ * SIMINT_B200_PREC_MIXED); 0 restores the default rule).
  * Returns SIMINT_B200_ERR_ARG when the variant does not exist for the class.
  * Sweep graphs captured earlier are rebuilt on their next use. */
 int simint_b200_set_variant(const int am[4], int deriv, int prec, int variant);
@@ -202,7 +235,10 @@ extern "C" {
  * owns.  simint_b200_compute_eri_noalloc then computes the same integrals
  * as simint_compute_eri_deriv(deriv, P, Q, ...) into the caller's device
  * buffer dev_integrals, on `stream` (cudaStream_t; NULL = legacy stream),
- * asynchronously.  It runs the cooperative kernel; its working memory is a
+ * asynchronously, in FP64 whatever simint_b200_set_precision says.  It runs
+ * the first cooperative kernel (classes whose shared-memory plan exceeds
+ * 200 KB -- the largest g classes -- return SIMINT_B200_ERR_CLASS); its
+ * working memory is a
  * file-scope static device array of simint_b200_noalloc_scratch_bytes()
  * (32 MiB) that every GPU which loads the library holds until exit, plus
  * static Boys tables and an identity ket order (at most 2^20 ket pairs).

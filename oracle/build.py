@@ -165,4 +165,5 @@ def build_ref(force=False, ref=None):
 
 if __name__ == "__main__":
     print(build_oracle(force=True))
+    print(build_oracle_ld(force=True))
     print(build_ref(force=True, ref=sys.argv[1] if len(sys.argv) > 1 else None))

@@ -76,14 +76,14 @@ def build_examples(ref):
     # the reference's own output of the same program
     sys.path.insert(0, HERE)
     import build_reflib
-    src = os.path.join(OUT, "src_gamess_l3")
+    src = build_reflib.src_dir("gamess_l3")
     refout = os.path.join(OUT, "example1_ref.out")
-    refbin = os.path.join(OUT, "example1_ref")
+    refbin = os.path.join(build_reflib.BUILD, "example1_ref")
     lib = build_reflib.lib_path("gamess_l3", "avx512")
     if not os.path.exists(lib):
         lib = build_reflib.lib_path("gamess_l3", "avx2")
     if os.path.exists(lib) and _stale(refout, [ex, lib]):
-        stage = os.path.join(OUT, "stage_gamess_l3_" + ("avx512" if "avx512" in lib else "avx2"))
+        stage = build_reflib.stage_dir("gamess_l3", "avx512" if "avx512" in lib else "avx2")
         _run(["gcc", "-std=gnu11", "-O2", "-I", src, "-I", stage, "-o", refbin, ex, lib,
               "-Wl,-rpath," + OUT, "-fopenmp", "-lm"])
         with open(refout, "w") as f:

@@ -14,7 +14,7 @@ builds exactly that, without the reference's CMake:
    (Ordering_GAMESS.cpp or Ordering_Psi4.cpp; generator/CMakeLists.txt:49-55
    picks one the same way);
 2. create.py run with those programs (create.py:85-96 options) into
-   oracle/_ref/src_<variant>/ -- it copies skel/ there and writes the
+   oracle/_ref/build/src_<variant>/ -- it copies skel/ there and writes the
    generated sources, the file lists and ostei_config.h.in;
 3. the two configuration headers CMake would write (vector_config.h with the
    vectorisation define, skel/CMakeLists.txt:51-59 and DefaultFlags.cmake;
@@ -55,6 +55,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+BUILD = os.path.join(OUT, "build")      # generator, sources and objects (not needed at run time)
 
 VARIANTS = {
     # name: (ordering, inline, max_am, deriv)
@@ -88,7 +89,7 @@ def _run(cmd, cwd=None, log=None):
 
 def build_generator(ref, ordering, jobs):
     """generator binaries for one ordering -> oracle/_ref/gen_<ordering>/"""
-    gdir = os.path.join(OUT, "gen_" + ordering.lower())
+    gdir = os.path.join(BUILD, "gen_" + ordering.lower())
     progs = ["ostei_generator", "ostei_deriv1_generator", "ostei_vrr_generator",
              "ostei_hrr_generator"]
     if all(os.path.exists(os.path.join(gdir, p)) for p in progs):
@@ -119,7 +120,7 @@ def build_generator(ref, ordering, jobs):
 def generate(ref, name, jobs):
     """create.py output for one variant -> oracle/_ref/src_<name>/"""
     ordering, inline, max_am, deriv = VARIANTS[name]
-    src = os.path.join(OUT, "src_" + name)
+    src = os.path.join(BUILD, "src_" + name)
     stamp = os.path.join(src, ".generated")
     if os.path.exists(stamp):
         return src
@@ -131,15 +132,15 @@ def generate(ref, name, jobs):
     if inline:
         cmd += ["-ve", "100", "-vg", "100", "-he", "100", "-hg", "100"]
     cmd.append(src)
-    os.makedirs(OUT, exist_ok=True)
-    _run(cmd, log=os.path.join(OUT, "create_%s.log" % name))
+    os.makedirs(BUILD, exist_ok=True)
+    _run(cmd, log=os.path.join(BUILD, "create_%s.log" % name))
     open(stamp, "w").close()
     return src
 
 
 def _config_headers(src, name, isa):
     ordering, inline, max_am, deriv = VARIANTS[name]
-    stage = os.path.join(OUT, "stage_%s_%s" % (name, isa))
+    stage = os.path.join(BUILD, "stage_%s_%s" % (name, isa))
     vc = os.path.join(stage, "simint", "vectorization", "vector_config.h")
     oc = os.path.join(stage, "simint", "ostei", "ostei_config.h")
     os.makedirs(os.path.dirname(vc), exist_ok=True)
@@ -150,6 +151,14 @@ def _config_headers(src, name, isa):
     with open(oc, "w") as f:
         f.write(tmpl.replace("@SIMINT_MAXAM@", str(max_am)).replace("@SIMINT_MAXDER@", str(deriv)))
     return stage
+
+
+def src_dir(name):
+    return os.path.join(BUILD, "src_" + name)
+
+
+def stage_dir(name, isa):
+    return os.path.join(BUILD, "stage_%s_%s" % (name, isa))
 
 
 def lib_path(name, isa):
@@ -164,7 +173,7 @@ def compile_lib(ref, name, isa, jobs):
     ordering, inline, max_am, deriv = VARIANTS[name]
     src = generate(ref, name, jobs)
     stage = _config_headers(src, name, isa)
-    objdir = os.path.join(OUT, "obj_%s_%s" % (name, isa))
+    objdir = os.path.join(BUILD, "obj_%s_%s" % (name, isa))
     os.makedirs(objdir, exist_ok=True)
     lst = open(os.path.join(src, "simint", "ostei", "gen",
                             "filelist_d%d_%d" % (deriv, max_am))).read().split()

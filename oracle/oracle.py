@@ -16,10 +16,20 @@ from simint_b200.capi import ShellP, PairP, declare_shell_api  # noqa: E402
 _dp = C.POINTER(C.c_double)
 
 
+def _recipe():
+    """oracle/build.py, loaded by path (another build.py may be first on
+    sys.path)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_build_recipe", os.path.join(HERE, "build.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
 def load_oracle():
     path = os.path.join(HERE, "liboracle.so")
     if not os.path.exists(path):
-        from build import build_oracle  # noqa
+        _recipe().build_oracle()
         build_oracle()
     lib = C.CDLL(path)
     lib.oracle_create_pair.argtypes = [C.c_int, ShellP, PairP, C.c_int]
@@ -54,8 +64,7 @@ def load_oracle_ld():
     oracle_compute_eri writes long double values."""
     path = os.path.join(HERE, "liboracle_ld.so")
     if not os.path.exists(path):
-        from build import build_oracle_ld  # noqa
-        build_oracle_ld()
+        _recipe().build_oracle_ld()
     lib = C.CDLL(path)
     lib.oracle_compute_eri.argtypes = [PairP, PairP, C.c_double, C.c_int, C.c_int, C.c_void_p]
     lib.oracle_compute_eri.restype = C.c_int

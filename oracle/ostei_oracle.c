@@ -732,6 +732,13 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
     real F[64];
     const int bra_on_A = ci.brastep_j, ket_on_C = ci.ketstep_l;
 
+    /* The reference's (ss|ss) kernel zeroes the screening values past the
+     * last ket primitive before testing a partial vector
+     * (skel/ostei_s_s_s_s.c): with a clipped ket list its vector test ends
+     * at the clip. */
+    int qclip_end = 0x7fffffff;
+    if(!P->am1 && !P->am2 && !Q->am1 && !Q->am2 && Q->nshell12_clip < Q->nshell12 && Q->nshell12_clip > 0)
+        qclip_end = qst[Q->nshell12_clip - 1] + Q->nprim12[Q->nshell12_clip - 1];
     for(int ab = 0; ab < P->nshell12_clip; ab++)
     for(int cd = 0; cd < Q->nshell12_clip; cd++)
     {
@@ -747,7 +754,7 @@ int oracle_compute_eri(struct simint_multi_shellpair const * P,
                     /* 8-wide vector test: [8*(j/8), 8*(j/8)+8) of the padded ket */
                     const int v0 = j & ~7;
                     double vmax = 0.0;
-                    for(int jj = v0; jj < v0 + 8; jj++)
+                    for(int jj = v0; jj < v0 + 8 && jj < qclip_end; jj++)
                     {
                         const double s = P->screen[i] * Q->screen[jj];
                         if(s > vmax) vmax = s;

@@ -26,6 +26,16 @@ static struct simint_shell * g_sh = NULL;
 static int g_nsh = 0;
 static struct simint_multi_shellpair ** g_ps = NULL;
 static int g_nps = 0, g_cps = 0;
+/* Per pair-set handle: a copy of the screening values of an (s s) pair set
+ * as created (NULL for other sets).  The reference's (ss|ss) kernel
+ * (skel/ostei_s_s_s_s.c) writes zeros into Q.screen past the last ket
+ * primitive when it tests a partial vector; with a clipped ket list
+ * (nshell12_clip < nshell12) those are the next pairs' values, so a later
+ * call that reaches further into the same list skips primitives it should
+ * not.  rd_rows keeps the shared pair sets as created: rows that evaluate
+ * into `out` run such calls on a private copy of the values, and timed runs
+ * put the values back after the loop. */
+static double ** g_scr0 = NULL;
 
 static double wtime(void)
 {
@@ -91,10 +101,10 @@ void rd_shell_schwarz(int npair, const int * pairs, double * out, int nthreads)
         out[p] = simint_shellscreen_schwarz(&g_sh[pairs[2 * p]], &g_sh[pairs[2 * p + 1]]);
 }
 
-/* A multi shell pair over an explicit pair list; returns its handle. */
-int rd_pairset(int npair, const int * pairs, int screen_method)
+/* Room for `need` handles. */
+static int reserve_handles(int need)
 {
-    if(g_nps == g_cps)
+    while(g_cps < need)
     {
         int nc = g_cps ? 2 * g_cps : 64;
         struct simint_multi_shellpair ** np =
@@ -102,8 +112,61 @@ int rd_pairset(int npair, const int * pairs, int screen_method)
         if(!np)
             return -1;
         g_ps = np;
+        double ** ns = (double **)realloc(g_scr0, sizeof(*ns) * (size_t)nc);
+        if(!ns)
+            return -1;
+        g_scr0 = ns;
         g_cps = nc;
     }
+    return 0;
+}
+
+/* Padded primitive slots of a pair set (the reference's layout: each batch
+ * of SIMINT_NSHELL_SIMD pairs rounded up to SIMINT_SIMD_LEN). */
+static int padded_slots(const struct simint_multi_shellpair * P)
+{
+    int idx = 0;
+    for(int p = 0; p < P->nshell12; p++)
+    {
+        idx += P->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 || p + 1 >= P->nshell12)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    return idx;
+}
+
+static double * screen_copy(const struct simint_multi_shellpair * P)
+{
+    if(P->am1 != 0 || P->am2 != 0 || !P->screen)
+        return NULL;
+    const size_t n = (size_t)padded_slots(P);
+    double * c = (double *)malloc(sizeof(double) * (n ? n : 1));
+    if(c)
+        memcpy(c, P->screen, sizeof(double) * n);
+    return c;
+}
+
+/* End (padded primitive index) of the last ket pair of a clipped (ss|ss)
+ * call, or -1 when the call is not one. */
+static int ssss_clip_end(const struct simint_multi_shellpair * P, const struct simint_multi_shellpair * Q)
+{
+    if(P->am1 || P->am2 || Q->am1 || Q->am2 || Q->nshell12_clip >= Q->nshell12 || Q->nshell12_clip <= 0)
+        return -1;
+    int idx = 0;
+    for(int p = 0; p < Q->nshell12_clip; p++)
+    {
+        idx += Q->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 && p + 1 < Q->nshell12_clip)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    return idx;
+}
+
+/* A multi shell pair over an explicit pair list; returns its handle. */
+int rd_pairset(int npair, const int * pairs, int screen_method)
+{
+    if(reserve_handles(g_nps + 1) != 0)
+        return -1;
     struct simint_shell * AB = (struct simint_shell *)malloc(sizeof(struct simint_shell) * 2 * (size_t)npair);
     struct simint_multi_shellpair * P = (struct simint_multi_shellpair *)malloc(sizeof(*P));
     if(!AB || !P)
@@ -121,6 +184,7 @@ int rd_pairset(int npair, const int * pairs, int screen_method)
     simint_create_multi_shellpair2(npair, AB, P, screen_method);
     free(AB);
     g_ps[g_nps] = P;
+    g_scr0[g_nps] = screen_copy(P);
     return g_nps++;
 }
 
@@ -128,16 +192,8 @@ int rd_pairset(int npair, const int * pairs, int screen_method)
  * are first, first+1, ... (returns first). */
 int rd_pairsets_single(int npair, const int * pairs, int screen_method, int nthreads)
 {
-    while(g_cps < g_nps + npair)
-    {
-        int nc = g_cps ? 2 * g_cps : 64;
-        struct simint_multi_shellpair ** np =
-            (struct simint_multi_shellpair **)realloc(g_ps, sizeof(*np) * (size_t)nc);
-        if(!np)
-            return -1;
-        g_ps = np;
-        g_cps = nc;
-    }
+    if(reserve_handles(g_nps + npair) != 0)
+        return -1;
     const int first = g_nps;
 #ifdef _OPENMP
     #pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads > 0 ? nthreads : 1)
@@ -151,6 +207,7 @@ int rd_pairsets_single(int npair, const int * pairs, int screen_method, int nthr
         simint_initialize_multi_shellpair(P);
         simint_create_multi_shellpair2(1, AB, P, screen_method);
         g_ps[first + p] = P;
+        g_scr0[first + p] = NULL;        /* one pair: never clipped */
     }
     g_nps += npair;
     return first;
@@ -160,16 +217,8 @@ int rd_pairsets_single(int npair, const int * pairs, int screen_method, int nthr
  * OpenMP over sets; handles first, first+1, ... (returns first). */
 int rd_pairsets_multi(int nset, const int * counts, const int * pairs, int screen_method, int nthreads)
 {
-    while(g_cps < g_nps + nset)
-    {
-        int nc = g_cps ? 2 * g_cps : 64;
-        struct simint_multi_shellpair ** np =
-            (struct simint_multi_shellpair **)realloc(g_ps, sizeof(*np) * (size_t)nc);
-        if(!np)
-            return -1;
-        g_ps = np;
-        g_cps = nc;
-    }
+    if(reserve_handles(g_nps + nset) != 0)
+        return -1;
     const int first = g_nps;
     long long * start = (long long *)malloc(sizeof(long long) * (size_t)(nset + 1));
     start[0] = 0;
@@ -192,6 +241,7 @@ int rd_pairsets_multi(int nset, const int * counts, const int * pairs, int scree
         simint_create_multi_shellpair2(n, AB, P, screen_method);
         free(AB);
         g_ps[first + s] = P;
+        g_scr0[first + s] = screen_copy(P);
     }
     free(start);
     g_nps += nset;
@@ -204,6 +254,8 @@ void rd_pairsets_free(void)
     {
         simint_free_multi_shellpair(g_ps[k]);
         free(g_ps[k]);
+        free(g_scr0[k]);
+        g_scr0[k] = NULL;
     }
     g_nps = 0;
 }
@@ -238,6 +290,9 @@ static long long count_primq(const struct simint_multi_shellpair * P,
     const int check = tol > 0.0 && P->screen && Q->screen;
     if(tol > 0.0 && P->screen_max * Q->screen_max < tol2)
         return 0;
+    /* the (ss|ss) kernel tests the vector at the clip with zeros past it */
+    const int cend = ssss_clip_end(P, Q);
+    const int qend = cend >= 0 ? cend : 0x7fffffff;
     long long n = 0;
     int istart = 0;
     for(int ab = 0; ab < P->nshell12_clip; ++ab)
@@ -260,7 +315,7 @@ static long long count_primq(const struct simint_multi_shellpair * P,
                     if(check)
                     {
                         double vmax = 0.0;
-                        for(int l = 0; l < SIMINT_SIMD_LEN; l++)
+                        for(int l = 0; l < SIMINT_SIMD_LEN && j + l < qend; l++)
                         {
                             const double v = P->screen[i] * Q->screen[j + l];
                             vmax = v > vmax ? v : vmax;
@@ -315,6 +370,8 @@ double rd_rows(int nrow, const int * bh, const int * kh, const int * kc, int der
     {
         double * work = (double *)SIMINT_ALLOC(wsz);
         double * scratch = out ? NULL : (double *)SIMINT_ALLOC(sizeof(double) * (size_t)maxsz);
+        double * scr = NULL;             /* private screening values (see g_scr0) */
+        size_t scr_cap = 0;
 #ifdef _OPENMP
         #pragma omp barrier
         #pragma omp master
@@ -329,6 +386,22 @@ double rd_rows(int nrow, const int * bh, const int * kh, const int * kc, int der
             if(kc[r] > 0 && kc[r] < Q.nshell12)
                 Q.nshell12_clip = kc[r];
             const struct simint_multi_shellpair * P = g_ps[bh[r]];
+            const int cend = (out && g_scr0[kh[r]] && tol > 0.0) ? ssss_clip_end(P, &Q) : -1;
+            if(cend >= 0)
+            {
+                const size_t n = (size_t)SIMINT_SIMD_ROUND(cend);
+                if(n > scr_cap)
+                {
+                    free(scr);
+                    scr = (double *)malloc(sizeof(double) * n);
+                    scr_cap = scr ? n : 0;
+                }
+                if(scr)
+                {
+                    memcpy(scr, g_scr0[kh[r]], sizeof(double) * n);
+                    Q.screen = scr;
+                }
+            }
             double * dst = out ? out + off[r] : scratch;
             const int rc = simint_compute_eri_deriv(deriv, P, &Q, tol, work, dst);
             if(rc < 0 && out)
@@ -343,6 +416,23 @@ double rd_rows(int nrow, const int * bh, const int * kh, const int * kc, int der
         SIMINT_FREE(work);
         if(scratch)
             SIMINT_FREE(scratch);
+        free(scr);
+    }
+    if(!out && tol > 0.0)
+    {
+        /* timed runs call the reference as it is: put back what its (ss|ss)
+         * kernel overwrote (each (s s) ket set once) */
+        char * done = (char *)calloc((size_t)(g_nps > 0 ? g_nps : 1), 1);
+        for(int r = 0; r < nrow && done; r++)
+        {
+            const struct simint_multi_shellpair * Q = g_ps[kh[r]];
+            if(g_scr0[kh[r]] && Q->screen && !done[kh[r]])
+            {
+                memcpy(Q->screen, g_scr0[kh[r]], sizeof(double) * (size_t)padded_slots(Q));
+                done[kh[r]] = 1;
+            }
+        }
+        free(done);
     }
     return t1 - t0;
 }

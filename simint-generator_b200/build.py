@@ -43,7 +43,11 @@ def _compile(src, obj, headers, verbose):
         return src, 0.0, ""
     t0 = time.time()
     if src.endswith(".cu"):
-        cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+        # generated kernels go without line tables (they would triple the
+        # library's size); the hand-written sources keep them for profiling
+        lineinfo = [] if os.path.dirname(src) == GEN else ["-lineinfo"]
+        cmd = [NVCC] + ARCH + ["-O3"] + lineinfo + ["-std=c++17", "-Xcompiler", "-fPIC",
+                               "-diag-suppress", "177",
                                "-I", os.path.join(REPO, "include"), "-I", CSRC,
                                "--expt-relaxed-constexpr", "--extended-lambda",
                                "-Xptxas", "-v" if verbose else "-O3",
@@ -65,7 +69,7 @@ def build(max_am=4, limit=DEFAULT_LIMIT, jobs=None, verbose=False, only=None):
     gen_files, classes = generate(GEN, max_am=max_am, limit=limit, only=only)
     # drop stale generated kernels of classes no longer selected
     keep = set(os.path.basename(f) for f in gen_files)
-    for f in glob.glob(os.path.join(GEN, "ostei_*.cu")):
+    for f in glob.glob(os.path.join(GEN, "ostei_*.cu")) + glob.glob(os.path.join(GEN, "col_*.cu")):
         if os.path.basename(f) not in keep:
             os.remove(f)
     headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) \
@@ -83,10 +87,18 @@ def build(max_am=4, limit=DEFAULT_LIMIT, jobs=None, verbose=False, only=None):
         work.append((s, obj))
     logs = []
     # generated kernels include only the device header and the kernel table
+    # (straight-line) or the column kernel's headers
     gen_headers = [os.path.join(CSRC, "ostei_device.cuh"), os.path.join(CSRC, "kernels.h")]
+    col_headers = gen_headers + [os.path.join(CSRC, h) for h in ("colkern.cuh", "coop2.cuh", "cartinfo.cuh")] \
+        + [os.path.join(REPO, "include", "simint_b200.h")]
+
+    def deps(s):
+        if os.path.dirname(s) != GEN:
+            return headers
+        return col_headers if os.path.basename(s).startswith("col_") else gen_headers
+
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        futs = [ex.submit(_compile, s, o, gen_headers if os.path.dirname(s) == GEN else headers, verbose)
-                for s, o in work]
+        futs = [ex.submit(_compile, s, o, deps(s), verbose) for s, o in work]
         for f in futs:
             src, dt, err = f.result()
             if dt > 0:

@@ -76,10 +76,9 @@ static inline int ci_flat(int i, int j, int k)
     return ci_lev_off(l) + ((l - i) * (l - i + 1)) / 2 + k;
 }
 
-// The table on the host (the same contents the device copy gets).
-static std::vector<CartInfo> cart_table_host()
+// Fill t[0 .. CI_NCART) with the table (no allocation).
+static void cart_table_fill(CartInfo * t)
 {
-    std::vector<CartInfo> t(CI_NCART);
     for(int l = 0; l <= CI_MAXL; l++)
     {
         int p = 0;
@@ -109,6 +108,13 @@ static std::vector<CartInfo> cart_table_host()
                 c.m2 = (short)(dir >= 0 ? ci_flat(q[0], q[1], q[2]) : -1);
             }
     }
+}
+
+// The table on the host (the same contents the device copy gets).
+static std::vector<CartInfo> cart_table_host()
+{
+    std::vector<CartInfo> t(CI_NCART);
+    cart_table_fill(t.data());
     return t;
 }
 

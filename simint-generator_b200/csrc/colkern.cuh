@@ -1,0 +1,435 @@
+// Column kernel: one CTA per shell quartet, one thread per (bra Cartesian
+// function, primitive quartet of a batch), the ket recursion of a thread's
+// bra function held in registers.
+//
+// Why: the table-driven cooperative kernel (coop2.cu) keeps every VRR
+// intermediate in shared memory, so each 4-FMA step costs five or more
+// shared-memory accesses and the kernel is bound by shared-memory bandwidth
+// and latency.  Here a thread owns the column (g_e, 0 | f)^(m) of one bra
+// function g_e over all ket functions f; three of the four source terms of a
+// ket step are the thread's own registers and only the (e-1_y, f-1_y)^(m+1)
+// term is read from another thread, so a step is ~5 FP64 operations and at
+// most one shared-memory load and one store.
+//
+// Per shell quartet: the surviving primitive quartets (the reference's
+// primitive screening, in order; in mixed mode split into an FP64 and an FP32
+// list by the error gate) are set up 64 at a time (set-up and Boys, one
+// thread each, into shared memory: col_setup) and processed in batches of NP:
+//   1. the bra-only recursion (g_e, 0|0)^(m), level by level (col_f0),
+//   2. the ket stages f = 1..c+d (generated per class: CT::stages), the top
+//      quartets summed into per-thread FP64 registers;
+// then the per-thread sums are added over the batch slots in a fixed order
+// into the cooperative kernel's accumulator layout, and its HRR
+// (c2_hrr_side, OSTEI_HRR_Algorithm_Base.cpp:160-283) runs in shared memory
+// and writes through the output index table (ordering and role swaps).
+// Shell quartets come from the launch's work queue (cta_next_task).
+//
+// Class constants, shared-memory sizes and the stage code come from a
+// generated traits struct CT (simint_b200/gen/colgen.py).
+#pragma once
+
+#include <vector>
+
+#include "coop2.cuh"
+
+__device__ __forceinline__ double cfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float cfma(float a, float b, float c) { return fmaf(a, b, c); }
+
+// coefficient record of a set-up primitive quartet (doubles, rows of NS)
+enum { CC_XP = 0, CC_YP = 3, CC_XQ = 6, CC_YQ = 9, CC_ZP = 12, CC_ZQ = 13, CC_O2P = 14, CC_O2Q = 15,
+       CC_O2PQ = 16, CC_F = 17 };
+
+__host__ __device__ constexpr int col_lo(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
+__host__ __device__ constexpr int col_nt(int nrole, int np) { return ((nrole * np + 31) / 32) * 32; }
+// survivors set up at once (one thread each)
+__host__ __device__ constexpr int col_ns(int nrole, int np) { return col_nt(nrole, np) < 64 ? col_nt(nrole, np) : 64; }
+
+// Cartesian exponents of flat index g (levels in order, Psi4 order inside a
+// level) and its level.
+__device__ __forceinline__ void col_cart(int g, int & i, int & j, int & k, int & l)
+{
+    l = 0;
+    while(col_lo(l + 1) <= g)
+        l++;
+    int p = g - col_lo(l);
+    for(i = l; i >= 0; i--)
+    {
+        const int n = l - i + 1;             // functions with this x exponent
+        if(p < n)
+            break;
+        p -= n;
+    }
+    k = p;
+    j = l - i - k;
+}
+
+__device__ __forceinline__ int col_flat(int i, int j, int k)
+{
+    const int l = i + j + k;
+    return col_lo(l) + ((l - i) * (l - i + 1)) / 2 + k;
+}
+
+__device__ __forceinline__ int col_stepdir(int i, int j, int k)
+{
+    const int e[3] = {i, j, k};
+    int mn = 1000;
+    for(int x = 0; x < 3; x++)
+        if(e[x] > 0 && e[x] < mn) mn = e[x];
+    for(int x = 2; x >= 0; x--)
+        if(e[x] == mn) return x;
+    return 0;
+}
+
+// Set-up and Boys values of survivors list[s0 .. s0 + NS) (NS threads in
+// parallel; slots past n get zeros, which run through the recursion as
+// zeros) into coef[k * NS + slot].
+template<class CT, int NS>
+__device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
+                                          int nj, unsigned long long njinv, bool fastdiv,
+                                          double * __restrict__ coef)
+{
+    const int tid = threadIdx.x;
+    if(tid < NS)
+    {
+        const int g = s0 + tid;
+        double v[CC_F + CT::L + 1];
+        #pragma unroll
+        for(int k = 0; k < CC_F + CT::L + 1; k++)
+            v[k] = 0.0;
+        if(g < n)
+        {
+            const int kk = list[g];
+            const int kq = fastdiv ? (int)(((unsigned long long)kk * njinv) >> 32) : kk / nj;
+            const int i = c.bi0 + kq, j = c.kj0 + (kk - kq * nj);
+            const BraPrim bp = load_bra_prim(c, i);
+            PrimSetup s;
+            prim_setup(c, bp, j, s);
+            v[CC_XP + 0] = s.PAx; v[CC_XP + 1] = s.PAy; v[CC_XP + 2] = s.PAz;
+            v[CC_YP + 0] = s.aopPQx; v[CC_YP + 1] = s.aopPQy; v[CC_YP + 2] = s.aopPQz;
+            v[CC_XQ + 0] = s.QCx; v[CC_XQ + 1] = s.QCy; v[CC_XQ + 2] = s.QCz;
+            v[CC_YQ + 0] = s.aoqPQx; v[CC_YQ + 1] = s.aoqPQy; v[CC_YQ + 2] = s.aoqPQz;
+            v[CC_ZP] = s.a_over_p; v[CC_ZQ] = s.a_over_q;
+            v[CC_O2P] = s.oo2p; v[CC_O2Q] = s.oo2q; v[CC_O2PQ] = s.oo2pq;
+            c2_boys(c.boys, s.T, CT::L, s.prefac, v + CC_F);
+        }
+        #pragma unroll
+        for(int k = 0; k < CC_F + CT::L + 1; k++)
+            coef[k * NS + tid] = v[k];
+    }
+    __syncthreads();
+}
+
+// Bra-only recursion of a batch: F0[(m * NROLE + g) * NP + slot] =
+// (g, 0 | 0)^(m) for every bra function g of levels 0..E, orders
+// 0..L - level (level 0: F_m times the pair prefactors).  Work items
+// (function, slot) of a level spread over the CTA; one barrier per level.
+template<typename T, class CT, int NP, int NT, int NS>
+__device__ __forceinline__ void col_f0(T * __restrict__ F0, const double * __restrict__ coef)
+{
+    constexpr int RS = CT::NROLE * NP;
+    const int tid = threadIdx.x;
+    if(tid < NP)
+    {
+        #pragma unroll
+        for(int m = 0; m <= CT::L; m++)
+            F0[m * RS + tid] = (T)coef[(CC_F + m) * NS + tid];
+    }
+    __syncthreads();
+    #pragma unroll
+    for(int e = 1; e <= CT::E; e++)
+    {
+        const int nitem = ((e + 1) * (e + 2) / 2) * NP;
+        for(int it = tid; it < nitem; it += NT)
+        {
+            const int pe = it / NP, slot = it - pe * NP;
+            int i, j, k, l;
+            col_cart(col_lo(e) + pe, i, j, k, l);
+            const int x = col_stepdir(i, j, k);
+            int q[3] = {i, j, k};
+            const int n = q[x] - 1;
+            q[x] -= 1;
+            const int g1 = col_flat(q[0], q[1], q[2]);
+            q[x] -= 1;
+            const int g2 = n > 0 ? col_flat(q[0], q[1], q[2]) : 0;
+            const T XP = (T)coef[(CC_XP + x) * NS + slot];
+            const T YP = (T)coef[(CC_YP + x) * NS + slot];
+            const T Zp = (T)coef[CC_ZP * NS + slot];
+            const T k2 = (T)((double)n * coef[CC_O2P * NS + slot]);
+            const T * s1 = F0 + g1 * NP + slot;
+            const T * s2 = F0 + g2 * NP + slot;
+            T * dst = F0 + (col_lo(e) + pe) * NP + slot;
+            #pragma unroll
+            for(int m = 0; m <= CT::L - e; m++)
+            {
+                T r = XP * s1[m * RS];
+                r = cfma(YP, s1[(m + 1) * RS], r);
+                if(n > 0)
+                    r = cfma(k2, cfma(Zp, s2[(m + 1) * RS], s2[m * RS]), r);
+                dst[m * RS] = r;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One batch of NP set-up survivors (coef: the first member's record, row
+// stride NS) in type T.
+template<typename T, class CT, int NP, int NT, int NS>
+__device__ __forceinline__ void col_batch(const double * __restrict__ coef, double * __restrict__ V,
+                                          int role, int slot, bool valid, const int (&loff)[3],
+                                          const int (&ny)[3], double (&acc)[CT::NTOP])
+{
+    T * F0 = (T *)V;
+    T * SB = F0;                                            // stage 2, 4, ... (F0 is dead by then)
+    T * SA = F0 + (CT::F0N > CT::SBN ? CT::F0N : CT::SBN) * NP;
+    col_f0<T, CT, NP, NT, NS>(F0, coef);
+    T XQ[3], YQ[3], cB[3], kq[CT::KQN], Zq = 0;
+    #pragma unroll
+    for(int y = 0; y < 3; y++)
+    {
+        XQ[y] = valid ? (T)coef[(CC_XQ + y) * NS + slot] : (T)0;
+        YQ[y] = valid ? (T)coef[(CC_YQ + y) * NS + slot] : (T)0;
+        cB[y] = valid ? (T)((double)ny[y] * coef[CC_O2PQ * NS + slot]) : (T)0;
+    }
+    if(valid)
+        Zq = (T)coef[CC_ZQ * NS + slot];
+    #pragma unroll
+    for(int k = 0; k < CT::KQN; k++)
+        kq[k] = valid ? (T)((double)(k + 1) * coef[CC_O2Q * NS + slot]) : (T)0;
+    CT::template stages<T, NP>(F0, SA, SB, role * NP + slot, loff, XQ, YQ, Zq, kq, cB, valid, acc);
+}
+
+template<class CT, int MODE, bool MIXED, int NP>
+__global__ void __launch_bounds__(col_nt(CT::NROLE, NP), 1)
+k_col(const KernArgs a, const C2Params p, const int vdoubles)
+{
+    constexpr int NT = col_nt(CT::NROLE, NP);
+    constexpr int NS = col_ns(CT::NROLE, NP);
+    extern __shared__ __align__(16) double sm[];
+    __shared__ int wcount[2][NT / 32];
+    __shared__ int s_cnt[2];
+    __shared__ long long s_qslot;
+    double * V = sm;
+    double * coef = sm + vdoubles;
+    double * acc2 = coef + (CC_F + CT::L + 1) * NS;
+    int * surv = (int *)(acc2 + ((p.acc_size + 1) & ~1));   // [0, NT): FP64 list, [NT, 2 NT): FP32 list
+    const int tid = threadIdx.x;
+    const int role = tid / NP, slot = tid - role * NP;
+    const bool valid = role < CT::NROLE;
+    int ri = 0, rj = 0, rk = 0, re = 0;
+    if(valid)
+        col_cart(role, ri, rj, rk, re);
+    const int ny[3] = {ri, rj, rk};
+    // shared-memory position of (g_e - 1_y) (own position when absent: its
+    // coefficient n_y(g_e) is then 0 and the value read is a finite one)
+    int loff[3];
+    #pragma unroll
+    for(int y = 0; y < 3; y++)
+    {
+        int q[3] = {ri, rj, rk};
+        q[y] -= 1;
+        loff[y] = (valid && ny[y] > 0 ? col_flat(q[0], q[1], q[2]) : (valid ? role : 0)) * NP + slot;
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    long long t = 0;
+    for(long long qslot = blockIdx.x; cta_next_task(a, qslot, t, &s_qslot); qslot += gridDim.x)
+    {
+        int iP, iQ;
+        long long off;
+        task_of<MODE>(a, t, iP, iQ, off);
+        QuartetCtx c;
+        make_ctx(a, iP, iQ, c);
+        const int ni = c.bi1 - c.bi0, nj = c.kj1 - c.kj0;
+        if(MIXED)
+        {
+            c.gL = CT::L;
+            c.gamp = hrr_amp(c, CT::A1, CT::A3);
+            // the gate bounds the error of one integral: each of the shell
+            // quartet's primitive quartets may take gate / (their number)
+            c.gate = a.gate / (double)max(1, ni * nj);
+        }
+        double acc[CT::NTOP];
+        #pragma unroll
+        for(int k = 0; k < CT::NTOP; k++)
+            acc[k] = 0.0;
+        const int ncand = ni * nj;
+        const unsigned long long njinv = nj > 0 ? (1ull << 32) / (unsigned)nj + 1ull : 0ull;
+        const bool fastdiv = (long long)ncand * nj < (1LL << 32);
+        for(int k0 = 0; k0 < ncand; k0 += NT)
+        {
+            // ordered compaction of the surviving candidates k0 .. k0 + NT
+            // (FP64 list; in mixed mode the gated ones go to the FP32 list)
+            const int k = k0 + tid;
+            bool ok = false, low = false;
+            if(k < ncand)
+            {
+                const int kq = fastdiv ? (int)(((unsigned long long)k * njinv) >> 32) : k / nj;
+                const int i = c.bi0 + kq, j = c.kj0 + (k - kq * nj);
+                const BraPrim bp = load_bra_prim(c, i);
+                ok = !(c.check && (bp.skip || !prim_survives(c, bp, j)));
+                if(MIXED && ok)
+                {
+                    PrimSetup s;
+                    prim_setup(c, bp, j, s);
+                    low = s.lowprec;
+                }
+            }
+            const bool hi = ok && !low, lo = ok && low;
+            const unsigned bh = __ballot_sync(0xffffffffu, hi);
+            const unsigned bl = __ballot_sync(0xffffffffu, lo);
+            if(lane == 0)
+            {
+                wcount[0][warp] = __popc(bh);
+                wcount[1][warp] = __popc(bl);
+            }
+            __syncthreads();
+            int b0 = 0, b1 = 0;
+            for(int w = 0; w < warp; w++)
+            {
+                b0 += wcount[0][w];
+                b1 += wcount[1][w];
+            }
+            const unsigned below = (1u << lane) - 1u;
+            if(hi)
+                surv[b0 + __popc(bh & below)] = k;
+            if(lo)
+                surv[NT + b1 + __popc(bl & below)] = k;
+            if(tid == NT - 1)
+            {
+                int t0 = 0, t1 = 0;
+                for(int w = 0; w < NT / 32; w++)
+                {
+                    t0 += wcount[0][w];
+                    t1 += wcount[1][w];
+                }
+                s_cnt[0] = t0;
+                s_cnt[1] = t1;
+            }
+            __syncthreads();
+            const int nhi = s_cnt[0], nlo = s_cnt[1];
+            if(MIXED && tid == 0 && nlo > 0 && a.fp32_count)
+                atomicAdd(a.fp32_count, (unsigned long long)nlo);
+            for(int s0 = 0; s0 < nhi; s0 += NS)
+            {
+                col_setup<CT, NS>(c, surv, s0, nhi, nj, njinv, fastdiv, coef);
+                for(int g0 = 0; g0 < NS && s0 + g0 < nhi; g0 += NP)
+                    col_batch<double, CT, NP, NT, NS>(coef + g0, V, role, slot, valid, loff, ny, acc);
+            }
+            if constexpr(MIXED)
+            {
+                for(int s0 = 0; s0 < nlo; s0 += NS)
+                {
+                    col_setup<CT, NS>(c, surv + NT, s0, nlo, nj, njinv, fastdiv, coef);
+                    for(int g0 = 0; g0 < NS && s0 + g0 < nlo; g0 += NP)
+                        col_batch<float, CT, NP, NT, NS>(coef + g0, V, role, slot, valid, loff, ny, acc);
+                }
+            }
+            __syncthreads();      // surv, s_cnt and wcount are reused
+        }
+        // sums over the batch slots, in slot order, into the accumulator
+        // layout of the HRR: acc2[(g_e - lo(a)) * NTOP + t]
+        constexpr int TOP0 = col_lo(CT::A0);
+        constexpr int NTR = CT::NROLE - TOP0;          // bra functions of levels a .. a+b
+        if(valid && role >= TOP0)
+        {
+            #pragma unroll
+            for(int k = 0; k < CT::NTOP; k++)
+                V[(k * NTR + (role - TOP0)) * NP + slot] = acc[k];
+        }
+        __syncthreads();
+        for(int idx = tid; idx < NTR * CT::NTOP; idx += NT)
+        {
+            const int k = idx / NTR, rr = idx - k * NTR;
+            double sum = 0.0;
+            #pragma unroll
+            for(int s2 = 0; s2 < NP; s2++)
+                sum += V[(k * NTR + rr) * NP + s2];
+            acc2[p.acc_off[0] + rr * p.acc_nf[0] + k] = sum;
+        }
+        __syncthreads();
+        // ---------------- HRR ----------------
+        double * LA = V + p.off_hrr_b;
+        double * LB = LA + p.hrr_layer;
+        double * mid = V + p.off_hrr_mid;
+        double * o = a.out + off;
+        const unsigned short * __restrict__ oidx = a.oidx;
+        const int * tt = p.tgt[0];
+        const int klo = tt[2];
+        const int ncol = c2_lev_off(tt[2] + tt[3] + 1) - c2_lev_off(klo);
+        const int nbra = c2_nc(tt[0]) * c2_nc(tt[1]);
+        const int nket = c2_nc(tt[2]) * c2_nc(tt[3]);
+        const int accb = p.acc_off[0], accnf = p.acc_nf[0];
+        const int e0 = c2_lev_off(p.elo[0]), f0 = c2_lev_off(p.flo[0]), fk = c2_lev_off(klo);
+        c2_hrr_side<NT>(p.brastep_j, p.hrr_nl[0][0], ncol, p.hrr_rows + p.hrr_base[0][0], p.hrr_loff[0][0],
+                        c.AB[0], c.AB[1], c.AB[2],
+                        [&](int g, int col) { return acc2[accb + (g - e0) * accnf + (fk + col - f0)]; },
+                        [&](int r, int col, double v) { mid[r * ncol + col] = v; }, LA, LB);
+        const int kl = c2_lev_off(klo);
+        c2_hrr_side<NT>(p.ketstep_l, p.hrr_nl[0][1], nbra, p.hrr_rows + p.hrr_base[0][1], p.hrr_loff[0][1],
+                        c.CD[0], c.CD[1], c.CD[2],
+                        [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
+                        [&](int r, int row, double v) { o[oidx[row * nket + r]] = v; }, LA, LB);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------
+// registry of the generated classes
+// ---------------------------------------------------------------------
+
+typedef void (*ColFn)(const KernArgs, const C2Params, const int);
+
+#define COL_NNP 2
+static constexpr int COL_NPS[COL_NNP] = {4, 8};
+
+struct ColKernels
+{
+    int am[4];
+    int L, nrole, ntop;
+    int vdoubles_per_np;                 // doubles of the F0|SA|SB region per batch slot
+    int red_per_np;                      // doubles of the slot-sum scratch per batch slot
+    int ncoef;                           // doubles of a coefficient record
+    int nt[COL_NNP];                     // threads per CTA for each NP
+    int ns[COL_NNP];                     // survivors set up at once for each NP
+    ColFn fn[COL_NNP][3][2];             // [np][mode][fp64, mixed]
+};
+
+struct ColTable
+{
+    std::vector<ColKernels> list;
+    void add(const ColKernels & k) { list.push_back(k); }
+};
+
+template<class CT, int NPI>
+static void col_fill_np(ColKernels & k)
+{
+    constexpr int NP = COL_NPS[NPI];
+    k.nt[NPI] = col_nt(CT::NROLE, NP);
+    k.ns[NPI] = col_ns(CT::NROLE, NP);
+    for(int md = 0; md < 3; md++)
+        k.fn[NPI][md][0] = k.fn[NPI][md][1] = nullptr;
+    if constexpr(col_nt(CT::NROLE, NP) <= 1024)
+    {
+        k.fn[NPI][0][0] = k_col<CT, 0, false, NP>;
+        k.fn[NPI][0][1] = k_col<CT, 0, true, NP>;
+        k.fn[NPI][1][0] = k_col<CT, 1, false, NP>;
+        k.fn[NPI][1][1] = k_col<CT, 1, true, NP>;
+        k.fn[NPI][2][0] = k_col<CT, 2, false, NP>;
+        k.fn[NPI][2][1] = k_col<CT, 2, true, NP>;
+    }
+}
+
+template<class CT>
+static void col_fill(ColKernels & k)
+{
+    k.L = CT::L;
+    k.nrole = CT::NROLE;
+    k.ntop = CT::NTOP;
+    k.vdoubles_per_np = (CT::F0N > CT::SBN ? CT::F0N : CT::SBN) + CT::SAN;
+    k.red_per_np = CT::NTOP * (CT::NROLE - col_lo(CT::A0));
+    k.ncoef = CC_F + CT::L + 1;
+    col_fill_np<CT, 0>(k);
+    col_fill_np<CT, 1>(k);
+}
+
+void simint_b200_register_col(ColTable & t);

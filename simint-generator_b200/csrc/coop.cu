@@ -633,35 +633,7 @@ int noalloc_setup(int dev)
        cudaMemcpyToSymbol(g_noalloc_boys, simint_b200_boys_longfac_host, sizeof(double) * 32,
                           sizeof(double) * 366 * 32) != cudaSuccess)
         return SIMINT_B200_ERR_CUDA;
-    for(int l = 0; l <= CI_MAXL; l++)
-    {
-        int p = 0;
-        for(int i = l; i >= 0; i--)
-            for(int j = l - i; j >= 0; j--, p++)
-            {
-                const int k = l - i - j;
-                CartInfo & c = g_noalloc_cart[ci_lev_off(l) + p];
-                c.ijk[0] = (signed char)i; c.ijk[1] = (signed char)j; c.ijk[2] = (signed char)k;
-                c.lev = (signed char)l;
-                c.pos = (signed char)p;
-                const int e[3] = {i, j, k};
-                int mn = 1000, dir = -1;
-                for(int x = 0; x < 3; x++)
-                    if(e[x] > 0 && e[x] < mn) mn = e[x];
-                for(int x = 2; x >= 0; x--)
-                    if(e[x] == mn) { dir = x; break; }
-                c.dir = (signed char)dir;
-                c.m1[0] = (short)ci_flat(i - 1, j, k);
-                c.m1[1] = (short)ci_flat(i, j - 1, k);
-                c.m1[2] = (short)ci_flat(i, j, k - 1);
-                c.p1[0] = (short)ci_flat(i + 1, j, k);
-                c.p1[1] = (short)ci_flat(i, j + 1, k);
-                c.p1[2] = (short)ci_flat(i, j, k + 1);
-                int q[3] = {i, j, k};
-                if(dir >= 0) q[dir] -= 2;
-                c.m2 = (short)(dir >= 0 ? ci_flat(q[0], q[1], q[2]) : -1);
-            }
-    }
+    cart_table_fill(g_noalloc_cart);
     if(cudaMemcpyToSymbol(c_cartinfo, g_noalloc_cart, sizeof(CartInfo) * CI_NCART) != cudaSuccess)
         return SIMINT_B200_ERR_CUDA;
     k_noalloc_iota<<<256, 256>>>(d.kord, NOALLOC_MAX_KETS);
@@ -677,15 +649,19 @@ int noalloc_setup(int dev)
 
 extern "C" size_t simint_b200_packed_size(struct simint_multi_shellpair const * P)
 {
+    if(!P)
+        return 0;
     sb200::PackedLayout L;
     return noalloc_layout(P, L);
 }
 
 extern "C" int simint_b200_pack(struct simint_multi_shellpair const * P, void * dst, size_t cap)
 {
+    if(!P || !dst)
+        return SIMINT_B200_ERR_ARG;
     sb200::PackedLayout L;
     const size_t need = noalloc_layout(P, L);
-    if(!P || !dst || cap < need)
+    if(cap < need)
         return SIMINT_B200_ERR_ARG;
     char * base = (char *)dst;
     double * rec = (double *)(base + L.off_rec);

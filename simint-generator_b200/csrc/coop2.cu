@@ -44,194 +44,7 @@
 #include "runtime.h"
 #include "cartinfo.cuh"
 
-#define C2_MAXL 10
-#define C2_MAXS 20
-#define C2_NCOEF 32          // per primitive quartet: 6 combos x 4, 1/2(p+q), 4 deriv weights, pad
-#define C2_SETUP 16          // primitive quartets set up in parallel
-#define C2_MAXN 225          // Cartesian pairs of (g g)
-
-enum { K_O2PQ = 24, K_W1 = 25 };
-
-// One VRR item, 16 bytes:
-//   x = dst | src1 << 16                  (offsets of the m = 0 slots in a wave buffer)
-//   y = src2 | src3 << 16                 (0 when absent)
-//   z = acc index of tag 0 (0xffff = none) | combo << 16 | has2 << 24 | has3 << 25
-//       | (mask of tags 1..4) << 26
-// One unit computes one auxiliary order m of one element (m is folded into
-// the offsets).
-//   w = nA | nB << 4 | gE << 8 | gF << 18 (integer factors; Cartesian indices of deriv tags)
-typedef int4 C2Item;
-
-struct C2Params
-{
-    int am[4];
-    int deriv, missing, ntarget, ntag, L, B;
-    int tgt[6][4];
-    int tgt_tag[6];
-    int brastep_j, ketstep_l;
-    int Emax, Fmax;
-    int elo[5], ehi[5], flo[5], fhi[5], acc_off[5], acc_nf[5], acc_size;
-    int wsize;                    // doubles per (wave, batch entry)
-    int smax;                     // last wavefront
-    int wstart[C2_MAXS + 2];      // item range of wavefront s: [wstart[s], wstart[s+1])
-    const C2Item * items;
-    int off_acc, off_prep, off_surv, off_hrr_b, off_hrr_mid;   // shared-memory layout (doubles)
-    int prep_stride;              // doubles per prepared primitive quartet
-    int off32;                    // offset (doubles) of its FP32 coefficient copy
-    int hrr_layer;                // doubles per HRR layer buffer
-    int smem_doubles;
-    int ordering;
-    int res_size;                 // deriv 1: doubles of all target results per CTA
-    int res_off[6];
-    const int2 * hrr_rows;        // HRR row tables (see c2_hrr_side)
-    int hrr_base[6][2];           // per target and side: first row
-    int hrr_loff[6][2][6];        // per target and side: row offsets of layers (relative)
-    int hrr_nl[6][2];             // per target and side: number of transfer layers
-};
-
-__device__ __forceinline__ int c2_lev_off(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
-__device__ __forceinline__ int c2_nc(int l) { return ((l + 1) * (l + 2)) / 2; }
-
-__device__ __forceinline__ int c2_index(const CartInfo * __restrict__ ci, int g, int ordering)
-{
-    const CartInfo & c = ci[g];
-    const int l = c.lev;
-    if(ordering == SIMINT_B200_ORDERING_GAMESS && (l == 2 || l == 3))
-    {
-        const int i = c.ijk[0], j = c.ijk[1], k = c.ijk[2];
-        if(l == 2)
-            return i == 2 ? 0 : j == 2 ? 1 : k == 2 ? 2 : (i == 1 && j == 1) ? 3 : i == 1 ? 4 : 5;
-        return i == 3 ? 0 : j == 3 ? 1 : k == 3 ? 2 : (i == 2 && j == 1) ? 3 : i == 2 ? 4
-             : (i == 1 && j == 2) ? 5 : j == 2 ? 6 : (i == 1 && k == 2) ? 7 : k == 2 ? 8 : 9;
-    }
-    return c.pos;
-}
-
-// One side of the HRR for every column at once, layer by layer in shared
-// memory.  in(g, col) gives the tops (functions on the top centre, levels
-// lo..lt); out(r, col, v) receives the (ta tb) block, r = pa * nc(tb) + pb.
-// rows[loff[sl-1] .. loff[sl]) describe layer sl, one int2 per row:
-// x = source A | source B << 16 (function indices on layer 1, rows of the
-// previous layer after), y = direction | output row << 2 (last layer).
-// Threads form a (row, column) grid.
-template<int NT, typename IN, typename OUT>
-__device__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * __restrict__ rows,
-                            const int * loff, double X0, double X1, double X2, IN in, OUT out,
-                            double * __restrict__ LA, double * __restrict__ LB)
-{
-    const int tid = threadIdx.x;
-    const int TC = ncol < NT ? ncol : NT;
-    const int TR = NT / TC;
-    const int tc = tid % TC, tr = tid / TC;
-    const double Xs[3] = {right_step ? X0 : -X0, right_step ? X1 : -X1, right_step ? X2 : -X2};
-    if(sl_max == 0)
-    {
-        // nothing to transfer: row r of the block is top function rows[r].x
-        const int nr = loff[0];
-        if(tr < TR)
-            for(int r = tr; r < nr; r += TR)
-            {
-                const int g = __ldg(&rows[r].x);
-                for(int col = tc; col < ncol; col += TC)
-                    out(r, col, in(g, col));
-            }
-        __syncthreads();
-        return;
-    }
-    double * dst = LA;
-    const double * src = LB;
-    for(int sl = 1; sl <= sl_max; sl++)
-    {
-        const int r0 = loff[sl - 1], r1 = loff[sl];
-        const bool last = sl == sl_max;
-        if(tr < TR)
-            #pragma unroll 2
-            for(int r = r0 + tr; r < r1; r += TR)
-            {
-                const int2 e = __ldg(&rows[r]);
-                const int a = e.x & 0xffff, b = (int)((unsigned)e.x >> 16);
-                const double X = Xs[e.y & 3];
-                const int orow = e.y >> 2;
-                if(sl == 1)
-                {
-                    for(int col = tc; col < ncol; col += TC)
-                    {
-                        const double v = fma(X, in(a, col), in(b, col));
-                        if(last) out(orow, col, v);
-                        else dst[(r - r0) * ncol + col] = v;
-                    }
-                }
-                else
-                {
-                    const double * sa = src + a * ncol;
-                    const double * sb = src + b * ncol;
-                    for(int col = tc; col < ncol; col += TC)
-                    {
-                        const double v = fma(X, sa[col], sb[col]);
-                        if(last) out(orow, col, v);
-                        else dst[(r - r0) * ncol + col] = v;
-                    }
-                }
-            }
-        __syncthreads();
-        double * t = (double *)src;
-        src = dst;
-        dst = t;
-    }
-}
-
-// Boys values F_0..F_L(T) times prefac into F (shared memory), the
-// reference's split: L < 4 every order from the Taylor grid (or the
-// asymptotic form for T >= 36.5), L >= 4 F_L then downward recursion
-// (boys.h:14-92, boys_taylor.h:14-39, boys_long.h:14-58).
-__device__ __forceinline__ void c2_boys(const double * __restrict__ tab, double T, int L, double prefac,
-                                        double * __restrict__ F)
-{
-    if(L < 4)
-    {
-        if(T >= 0.0 && T < 36.5)
-        {
-            const int idx = (int)(10.0 * (T + 0.05));
-            const double dx = (double)idx * 0.1 - T;
-            for(int n = 0; n <= L; n++)
-                F[n] = boys_taylor(tab + idx * 32 + n, dx) * prefac;
-        }
-        else
-        {
-            const double x1 = 1.0 / T;
-            double x2 = sqrt(x1);
-            for(int n = 0; n <= L; n++)
-            {
-                F[n] = (__ldg(tab + SB_BOYS_LONGFAC_OFF + n) * x2) * prefac;
-                x2 *= x1;
-            }
-        }
-        return;
-    }
-    double f;
-    if(T >= 0.0 && T < 36.5)
-    {
-        const int idx = (int)(10.0 * (T + 0.05));
-        const double dx = (double)idx * 0.1 - T;
-        f = boys_taylor(tab + idx * 32 + L, dx);
-    }
-    else
-        f = __ldg(tab + SB_BOYS_LONGFAC_OFF + L) * pow(T, -((double)L + 0.5));
-    const double x2 = 2.0 * T;
-    const double ex = exp(-T);
-    F[L] = f * prefac;
-    for(int n = L - 1; n >= 0; n--)
-    {
-        f = (1.0 / (2.0 * n + 1.0)) * fma(x2, f, ex);
-        F[n] = f * prefac;
-    }
-}
-
-// Small non-negative integer n as a floating-point value without a
-// conversion instruction: the bits of 2^52 + n (resp. 2^23 + n) minus 2^52
-// (2^23), exact for n < 2^23.
-__device__ __forceinline__ void c2_small(int n, double & d) { d = __hiloint2double(0x43300000, n) - 4503599627370496.0; }
-__device__ __forceinline__ void c2_small(int n, float & f) { f = __int_as_float(0x4b000000 | n) - 8388608.0f; }
+#include "coop2.cuh"
 
 // Coefficient combo of one prepared primitive quartet: X, Y, Z, 1/2s.
 __device__ __forceinline__ void c2_combo(const double * cf, int combo, double & X, double & Y, double & Z, double & O)
@@ -463,7 +276,9 @@ __global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT == 128 ? 4 : 2)) k_coop
     double * res = gres + (size_t)blockIdx.x * p.res_size;
     __syncthreads();
 
-    for(long long t = blockIdx.x; t < a.ntask; t += gridDim.x)
+    __shared__ long long s_qslot;
+    long long t = 0;
+    for(long long slot = blockIdx.x; cta_next_task(a, slot, t, &s_qslot); slot += gridDim.x)
     {
         int iP, iQ;
         long long off;
@@ -578,6 +393,8 @@ __global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT == 128 ? 4 : 2)) k_coop
                     s_slot[tid] = tid;
                 __syncthreads();
                 const int nhigh = MIXED ? s_nhigh : ng;
+                if(MIXED && tid == 0 && ng > nhigh && a.fp32_count)
+                    atomicAdd(a.fp32_count, (unsigned long long)(ng - nhigh));
                 // batches of up to 8 in FP64 (codes 2x, 4x, 6x: B = x); the
                 // 8-way batch dispatch also made the 2-wide batches of the
                 // largest classes 5-8 % faster than a 4-way one (measured)
@@ -1074,6 +891,7 @@ static bool c2_build(const int am[4], int deriv, int v, C2Host & h)
     // one intermediate buffer suffices up to two transfer steps per side
     const int nbuf = maxslm >= 3 ? 2 : (maxslm == 2 ? 1 : 0);
     p.hrr_layer = (hl + 1) & ~1;
+    p.hrr_need = nbuf * p.hrr_layer + midmax;
     // prepared primitive quartet: FP64 coefficients and Boys values, then an
     // FP32 copy of the coefficients (25 floats) for the mixed-precision VRR
     p.off32 = (C2_NCOEF + p.L + 1 + 1) & ~1;
@@ -1125,6 +943,43 @@ static C2Host * c2_get(const int am[4], int deriv, int v)
         it = g_c2.emplace(key, std::move(h)).first;
     }
     return &it->second;
+}
+
+// Device copies of the unit and HRR tables of plan h on the current device
+// (uploaded once per device); their addresses go into p.
+static bool c2_dev_tables(C2Host * h, C2Params & p)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_c2_mutex);
+    auto it = h->dev_tables.find(dev);
+    if(it == h->dev_tables.end())
+    {
+        const size_t bi = h->items.size() * sizeof(C2Item), bh = h->hrr.size() * sizeof(int2);
+        char * d = nullptr;
+        if(cudaMalloc(&d, std::max<size_t>(16, bi + bh)) != cudaSuccess)
+        {
+            cudaGetLastError();
+            set_error("out of device memory for cooperative-kernel tables");
+            return false;
+        }
+        cudaMemcpy(d, h->items.data(), bi, cudaMemcpyHostToDevice);
+        cudaMemcpy(d + bi, h->hrr.data(), bh, cudaMemcpyHostToDevice);
+        it = h->dev_tables.emplace(dev, d).first;
+    }
+    p.items = (const C2Item *)it->second;
+    p.hrr_rows = (const int2 *)(it->second + h->items.size() * sizeof(C2Item));
+    return true;
+}
+
+bool coop2_hrr_params(const int am[4], C2Params & out)
+{
+    C2Host * h = c2_get(am, 0, 0);
+    if(!h->ok)
+        return false;
+    upload_cart_info();
+    out = h->p;
+    return c2_dev_tables(h, out);
 }
 
 bool coop2_supported(const int am[4], int deriv, int v)
@@ -1183,29 +1038,9 @@ int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, 
         return SIMINT_B200_ERR_CLASS;
     }
     upload_cart_info();
-    int dev = 0;
-    cudaGetDevice(&dev);
     C2Params p = h->p;
-    {
-        std::lock_guard<std::mutex> lk(g_c2_mutex);
-        auto it = h->dev_tables.find(dev);
-        if(it == h->dev_tables.end())
-        {
-            const size_t bi = h->items.size() * sizeof(C2Item), bh = h->hrr.size() * sizeof(int2);
-            char * d = nullptr;
-            if(cudaMalloc(&d, std::max<size_t>(16, bi + bh)) != cudaSuccess)
-            {
-                cudaGetLastError();
-                set_error("out of device memory for cooperative-kernel tables");
-                return SIMINT_B200_ERR_CUDA;
-            }
-            cudaMemcpy(d, h->items.data(), bi, cudaMemcpyHostToDevice);
-            cudaMemcpy(d + bi, h->hrr.data(), bh, cudaMemcpyHostToDevice);
-            it = h->dev_tables.emplace(dev, d).first;
-        }
-        p.items = (const C2Item *)it->second;
-        p.hrr_rows = (const int2 *)(it->second + h->items.size() * sizeof(C2Item));
-    }
+    if(!c2_dev_tables(h, p))
+        return SIMINT_B200_ERR_CUDA;
     p.ordering = ordering();
     a.swapB = a.swapK = a.pq = 0;
     a.oidx = nullptr;

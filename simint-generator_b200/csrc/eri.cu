@@ -545,6 +545,8 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         count_launch(1);
         return 0;
     }
+    if(col_is_variant(v) && col_supported(req, deriv, v))
+        return launch_col(a, req, mode, prec, stream, v);
     if(coop2_is_variant(v) && coop2_supported(req, deriv, v))
         return launch_coop2(a, req, deriv, mode, prec, stream, v);
     if(v == VAR_COOP1 && coop_supported(req, deriv))
@@ -556,6 +558,60 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
     if(coop_supported(req, deriv))
         return launch_coop(a, req, deriv, mode, stream);
     return launch_generic(a, req, u, deriv, mode, stream);
+}
+
+// Whether launch_class runs class req on a CTA-per-quartet kernel that takes
+// its shell quartets from KernArgs::wq (the cooperative and column kernels):
+// the same choice of kernel as launch_class.
+bool class_uses_queue(const int req[4], int deriv, int prec)
+{
+    const UniqueMap u = unique_of(req);
+    const ClassKernels * k = deriv == 0 ? find_kernels(u) : nullptr;
+    int v = variant_of(req, deriv, prec);
+    if(v >= 100)
+        v -= 100;
+    if(v == VAR_DEFAULT)
+        v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
+    if((v == VAR_STRAIGHT || v == VAR_STRAIGHT64) && k)
+        return false;
+    if((v == VAR_WARP || v == VAR_WARP64) && k && k->fnw[2][0])
+        return false;
+    if(col_is_variant(v) && col_supported(req, deriv, v))
+        return true;
+    if(coop2_is_variant(v) && coop2_supported(req, deriv, v))
+        return true;
+    if(v == VAR_COOP1 && coop_supported(req, deriv))
+        return false;
+    if(v == VAR_GENERIC)
+        return false;
+    return coop2_supported(req, deriv);
+}
+
+// The reference's (ss|ss) kernel (skel/ostei_s_s_s_s.c) sets the screening
+// values of the lanes past the last ket primitive to zero before testing a
+// partial last vector -- in the caller's pair data: later calls that reach
+// further into the same ket list see the zeros.  For a ket list clipped
+// inside a vector (nshell12_clip < nshell12) the first call's test of that
+// vector therefore covers only its slots below the clip.  [v0, v1) are those
+// slots (padded primitive indices of Q), or an empty range when the call is
+// not (ss|ss), is not clipped or the clip ends on a vector boundary.  The
+// caller's data is left unchanged here.
+void ssss_clip_vector(const simint_multi_shellpair * P, const simint_multi_shellpair * Q, int & v0, int & v1)
+{
+    v0 = v1 = 0;
+    if(P->am1 || P->am2 || Q->am1 || Q->am2 || Q->nshell12_clip >= Q->nshell12 || Q->nshell12_clip <= 0)
+        return;
+    int idx = 0;
+    for(int p = 0; p < Q->nshell12_clip; p++)
+    {
+        idx += Q->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 && p + 1 < Q->nshell12_clip)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    if(idx % SIMINT_SIMD_LEN == 0)
+        return;
+    v0 = idx - idx % SIMINT_SIMD_LEN;
+    v1 = idx;
 }
 
 // Run one P x Q rectangle on the device.  dP/dQ already hold packed pair
@@ -580,6 +636,8 @@ int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
     a.gate = (prec == SIMINT_B200_PREC_MIXED) ? gatev : 0.0;
     a.out = dout;
     a.nout = nc * (deriv ? 12 : 1);
+    if(a.check)
+        ssss_clip_vector(P, Q, a.kvec0, a.kvec1);
     return launch_class(a, req, deriv, 0, prec, stream);
 }
 
@@ -962,8 +1020,18 @@ extern "C" long long simint_b200_count_primq(struct simint_multi_shellpair const
     pair_starts(Q, qs, npQ);
     std::vector<double> vmax((npQ + 7) / 8, 0.0);
     if(check)
+    {
         for(int j = 0; j < npQ; j++)
             vmax[j / 8] = std::max(vmax[j / 8], Q->screen[j]);
+        int v0, v1;
+        ssss_clip_vector(P, Q, v0, v1);
+        if(v1 > v0)
+        {
+            vmax[v0 / 8] = 0.0;
+            for(int j = v0; j < v1; j++)
+                vmax[v0 / 8] = std::max(vmax[v0 / 8], Q->screen[j]);
+        }
+    }
     long long n = 0;
     for(int ab = 0; ab < P->nshell12_clip; ab++)
         for(int i = ps[ab]; i < ps[ab] + P->nprim12[ab]; i++)
@@ -1086,6 +1154,12 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case 41: case 42: case 44: case 48:
         case 61: case 62: case 64: case 68:
             ok = coop2_supported(am, deriv, variant);
+            break;
+        case 81: case 82:
+            ok = col_supported(am, deriv, variant);
+            break;
+        case 181: case 182:
+            ok = prec == SIMINT_B200_PREC_MIXED && col_supported(am, deriv, variant - 100);
             break;
         case 121: case 122: case 124: case 128:
         case 141: case 142: case 144: case 148:

@@ -28,6 +28,21 @@ struct PairSetDev
     int npair;
 };
 
+// Device work queue of one launch.  Tasks 0 .. published-1 may be taken; a
+// CTA takes the next index with one atomic add.  When it runs past the
+// published count it waits for more -- at most spin_limit polls of about a
+// microsecond each -- or leaves once the queue is closed.  A wait that runs
+// out sets bit 0 of status (SIMINT_B200_ERR_TIMEOUT on the host) and the CTA
+// returns, so a producer that never finishes cannot hang the device.
+struct WorkQueue
+{
+    unsigned long long next;
+    unsigned long long published;
+    unsigned int closed;
+    unsigned int status;
+    unsigned long long spin_limit;
+};
+
 struct KernArgs
 {
     PairSetDev P, Q;          // requested bra and ket pair sets
@@ -53,7 +68,65 @@ struct KernArgs
     const int * korder;
     int nb;
     long long task0;
+    // CTA-per-quartet kernels: tasks handed out by a device work queue
+    // (nullptr: static grid-stride order), queue slot q running task
+    // tperm[q] (nullptr: q) -- the host orders a class's tasks by primitive
+    // count, heaviest first
+    WorkQueue * wq;
+    const int * tperm;
+    // mixed precision: primitive quartets the CTA-per-quartet kernels ran
+    // in FP32 are added here (nullptr: not counted)
+    unsigned long long * fp32_count;
+    // (ss|ss) with a clipped ket list: ket slots [kvec0, kvec1) are the
+    // partial last vector below the clip, whose vector test covers only
+    // them (empty range: no such vector)
+    int kvec0, kvec1;
 };
+
+// The next queue slot of the calling thread's CTA (thread 0 calls it), or -1
+// when the queue is drained or a wait ran out.
+__device__ __forceinline__ long long queue_pull(WorkQueue * q)
+{
+    const unsigned long long t = atomicAdd(&q->next, 1ull);
+    volatile WorkQueue * v = q;
+    for(unsigned long long it = 0;; it++)
+    {
+        if(t < v->published)
+            return (long long)t;
+        if(v->closed)
+        {
+            __threadfence();
+            return t < v->published ? (long long)t : -1;
+        }
+        if(it >= v->spin_limit)
+        {
+            atomicOr(&q->status, 1u);
+            return -1;
+        }
+        __nanosleep(1000);
+    }
+}
+
+// Task loop of a CTA-per-quartet kernel: static grid stride, or queue pulls.
+// Returns false when the CTA has no further task; t is the task index.
+__device__ __forceinline__ bool cta_next_task(const KernArgs & a, long long & slot, long long & t,
+                                              long long * s_slot)
+{
+    if(a.wq)
+    {
+        if(threadIdx.x == 0)
+            *s_slot = queue_pull(a.wq);
+        __syncthreads();
+        slot = *s_slot;
+        __syncthreads();
+        if(slot < 0)
+            return false;
+    }
+    else if(slot >= a.ntask)
+        return false;
+    t = a.tperm ? (long long)__ldg(a.tperm + slot) : slot;
+    return true;
+}
 
 struct QuartetCtx
 {
@@ -70,6 +143,8 @@ struct QuartetCtx
     double gamp;              // mixed precision: HRR growth (1+|AB|)^nb (1+|CD|)^nd
     const unsigned short * oidx;
     const double * boys;
+    int kvec0, kvec1;         // see KernArgs
+    unsigned long long * fp32_count;   // see KernArgs
 };
 
 struct BraPrim
@@ -197,11 +272,22 @@ __device__ __forceinline__ BraPrim load_bra_prim(const QuartetCtx & c, int i)
 
 // Screening test of ket primitive j against bra primitive bp (only called
 // when screening is on): the reference's 8-wide vector test, plus its
-// bra-level test when the requested bra set plays the ket role.
+// bra-level test when the requested bra set plays the ket role.  The
+// reference's (ss|ss) kernel zeroes the screening values of the lanes past
+// the last ket primitive before the test of a partial vector
+// (skel/ostei_s_s_s_s.c), so for a ket list clipped inside a vector the
+// test of that vector covers the slots below the clip only.
 __device__ __forceinline__ bool prim_survives(const QuartetCtx & c, const BraPrim & bp, int j)
 {
     const double * r = c.kprim + (size_t)j * SB_REC;
-    const double ks = r[13], kv = r[14];
+    const double ks = r[13];
+    double kv = r[14];
+    if(j >= c.kvec0 && j < c.kvec1)
+    {
+        kv = 0.0;
+        for(int s = c.kvec0; s < c.kvec1; s++)
+            kv = fmax(kv, c.kprim[(size_t)s * SB_REC + 13]);
+    }
     const double v = c.pq ? ks * bp.vecmax : bp.screen * kv;
     if(v < c.tol2)
         return false;
@@ -320,6 +406,9 @@ __device__ __forceinline__ void make_ctx(const KernArgs & a, int iP, int iQ, Qua
     c.gamp = 1.0;
     c.oidx = a.oidx;
     c.boys = a.boys;
+    c.kvec0 = a.kvec0;
+    c.kvec1 = a.kvec1;
+    c.fp32_count = a.fp32_count;
 }
 
 // Map a thread to a shell quartet.  MODE 0: the P x Q rectangle of

@@ -80,6 +80,8 @@ void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, do
 
 int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
                  cudaStream_t stream);
+bool class_uses_queue(const int req[4], int deriv, int prec);
+void ssss_clip_vector(const simint_multi_shellpair * P, const simint_multi_shellpair * Q, int & v0, int & v1);
 
 // Generic (table-driven, dense) kernel for classes without a straight-line
 // kernel and for deriv=1.  Everything in a except the role swaps is filled.
@@ -94,14 +96,19 @@ bool coop2_supported(const int am[4], int deriv, int v = 0);
 bool coop2_is_variant(int v);
 int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
                  int v = 0);
+// Column kernel (colkern.cuh), deriv 0: variant codes 81 (4 primitive
+// quartets per batch) and 82 (8).
+bool col_is_variant(int v);
+bool col_supported(const int req[4], int deriv, int v);
+int launch_col(KernArgs & a, const int req[4], int mode, int prec, cudaStream_t stream, int v);
 
 // Kernel variant per (requested class, deriv, precision), chosen by the
 // autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
 // 5 straight-line in FP64 even in mixed mode, 6 (7) straight-line with a
 // warp per shell quartet (in FP64 even in mixed mode), 20+B / 40+B / 60+B
-// cooperative v2 with batch B and 256 / 128 / 64 threads; 100 + a cooperative
-// code: that kernel
-// in FP64 even in mixed mode.
+// cooperative v2 with batch B and 256 / 128 / 64 threads, 81 / 82 column
+// kernel with 4 / 8 primitive quartets per batch; 100 + a cooperative or
+// column code: that kernel in FP64 even in mixed mode.
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5,
        VAR_WARP = 6, VAR_WARP64 = 7 };
 int variant_of(const int req[4], int deriv, int prec);

@@ -55,8 +55,35 @@ struct QClass
     long long offset = 0;
     std::vector<long long> prefix;   // nb + 1
     std::vector<int> border;         // bra pair of each b
-    DevBuf dev;                      // prefix, border
+    bool has_perm = false;           // task order by primitive count uploaded
+    DevBuf dev;                      // prefix, border, task order
 };
+
+// Tasks of a class up to this count get a heaviest-first visiting order.
+#define SWEEP_PERM_MAX (64LL << 20)
+// Per class in the basis' queue buffer: the work queue, then the counter of
+// primitive quartets run in FP32.
+#define SWEEP_QSTRIDE (sizeof(WorkQueue) + sizeof(unsigned long long))
+
+// A launch's queue: every task published and the queue closed (the status
+// word and the FP32 counter keep what earlier launches of the sweep left).
+__global__ void k_queue_reset(WorkQueue * q, long long ntask, unsigned long long spin_limit)
+{
+    q->next = 0;
+    q->published = (unsigned long long)ntask;
+    q->closed = 1;
+    q->spin_limit = spin_limit;
+}
+
+// A queue in a given state, for the probe of the bounded wait.
+__global__ void k_queue_set(WorkQueue * q, long long published, int closed, unsigned long long spin_limit)
+{
+    q->next = 0;
+    q->published = (unsigned long long)published;
+    q->closed = (unsigned)closed;
+    q->status = 0;
+    q->spin_limit = spin_limit;
+}
 
 __global__ void k_checksum(const double * __restrict__ v, long long n, double * __restrict__ sums)
 {
@@ -125,6 +152,7 @@ struct simint_b200_basis
     std::vector<QClass> qcs;
     long long total_out = 0;
     DevBuf dsums;
+    DevBuf dqueue;                         // per class: WorkQueue + FP32 counter (SWEEP_QSTRIDE)
     std::map<std::array<long long, 3>, cudaGraphExec_t> graphs;
     std::map<std::array<long long, 3>, int> eager_done;
     long long graph_epoch = -1;            // settings_epoch() the graphs were built under
@@ -151,16 +179,55 @@ static void layout_outputs(simint_b200_basis * b)
     }
 }
 
-static int upload_tasks(QClass & q)
+static size_t perm_offset(const QClass & q)
 {
     const size_t szp = (q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255;
-    if(!q.dev.reserve(szp + q.border.size() * sizeof(int) + 8))
+    return szp + ((q.border.size() * sizeof(int) + 255) & ~(size_t)255);
+}
+
+// Task lists of class q on the device: prefix, border and (up to
+// SWEEP_PERM_MAX tasks) the visiting order of the CTA-per-quartet kernels'
+// work queue -- tasks by decreasing primitive-pair product (a stable
+// counting sort), so the longest shell quartets start first and the short
+// ones fill the tail of the launch.
+static int upload_tasks(QClass & q, const PairClass & X, const PairClass & Y)
+{
+    const size_t szp = (q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255;
+    const size_t off = perm_offset(q);
+    q.has_perm = q.ntask > 0 && q.ntask <= SWEEP_PERM_MAX;
+    const size_t szperm = q.has_perm ? (size_t)q.ntask * sizeof(int) : 0;
+    if(!q.dev.reserve(off + szperm + 8))
     {
         set_error("out of memory building task lists");
         return SIMINT_B200_ERR_CUDA;
     }
     cudaMemcpy(q.dev.ptr, q.prefix.data(), q.prefix.size() * sizeof(long long), cudaMemcpyHostToDevice);
     cudaMemcpy((char *)q.dev.ptr + szp, q.border.data(), q.border.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if(q.has_perm)
+    {
+        int maxw = 1;
+        for(int ip : q.border)
+            maxw = std::max(maxw, X.P.nprim12[ip]);
+        int maxk = 1;
+        for(int iq = 0; iq < Y.P.nshell12; iq++)
+            maxk = std::max(maxk, Y.P.nprim12[iq]);
+        const int nkey = maxw * maxk + 1;
+        std::vector<long long> cnt(nkey + 1, 0);
+        auto key = [&](size_t r, long long i) {
+            return nkey - 1 - X.P.nprim12[q.border[r]] * Y.P.nprim12[Y.order[(size_t)i]];
+        };
+        for(size_t r = 0; r + 1 < q.prefix.size(); r++)
+            for(long long i = 0; i < q.prefix[r + 1] - q.prefix[r]; i++)
+                cnt[key(r, i) + 1]++;
+        for(int k = 0; k < nkey; k++)
+            cnt[k + 1] += cnt[k];
+        std::vector<int> perm((size_t)q.ntask);
+        long long t = 0;
+        for(size_t r = 0; r + 1 < q.prefix.size(); r++)
+            for(long long i = 0; i < q.prefix[r + 1] - q.prefix[r]; i++, t++)
+                perm[(size_t)cnt[key(r, i)]++] = (int)t;
+        cudaMemcpy((char *)q.dev.ptr + off, perm.data(), szperm, cudaMemcpyHostToDevice);
+    }
     return 0;
 }
 
@@ -310,7 +377,7 @@ extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simin
             q.nfull = tot;
             if(tot == 0)
                 continue;
-            if(upload_tasks(q) != 0)
+            if(upload_tasks(q, X, Y) != 0)
             {
                 simint_b200_basis_free(b);
                 return nullptr;
@@ -318,11 +385,14 @@ extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simin
             b->qcs.push_back(std::move(q));
         }
     layout_outputs(b);
-    if(!b->dsums.reserve(2 * sizeof(double) * std::max<size_t>(1, b->qcs.size())))
+    if(!b->dsums.reserve(2 * sizeof(double) * std::max<size_t>(1, b->qcs.size())) ||
+       !b->dqueue.reserve(SWEEP_QSTRIDE * std::max<size_t>(1, b->qcs.size())))
     {
+        set_error("out of device memory for the sweep's checksums and queues");
         simint_b200_basis_free(b);
         return nullptr;
     }
+    cudaMemset(b->dqueue.ptr, 0, SWEEP_QSTRIDE * std::max<size_t>(1, b->qcs.size()));
     cudaError_t e = cudaDeviceSynchronize();
     if(e != cudaSuccess)
     {
@@ -358,7 +428,7 @@ extern "C" int simint_b200_basis_subsample(simint_b200_basis * b, long long maxq
         q.border.swap(bor);
         q.ntask = q.prefix.back();
         q.nprimq = 0;
-        if(upload_tasks(q) != 0)
+        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky]) != 0)
             return SIMINT_B200_ERR_CUDA;
     }
     layout_outputs(b);
@@ -404,7 +474,7 @@ extern "C" int simint_b200_basis_subsample_stride(simint_b200_basis * b, int str
         q.border.swap(bor);
         q.ntask = q.prefix.back();
         q.nprimq = 0;
-        if(upload_tasks(q) != 0)
+        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky]) != 0)
             return SIMINT_B200_ERR_CUDA;
     }
     layout_outputs(b);
@@ -457,6 +527,7 @@ extern "C" void simint_b200_basis_free(simint_b200_basis * b)
         pc.dsh.release();
     b->daooff.release();
     b->dsums.release();
+    b->dqueue.release();
     for(int i = 0; i < SWEEP_SIDE; i++)
     {
         if(b->side[i]) cudaStreamDestroy(b->side[i]);
@@ -542,6 +613,20 @@ extern "C" int simint_b200_basis_class_quartets(simint_b200_basis const * b, int
     return 0;
 }
 
+static WorkQueue * class_queue(simint_b200_basis * b, size_t k)
+{
+    return (WorkQueue *)((char *)b->dqueue.ptr + k * SWEEP_QSTRIDE);
+}
+
+static unsigned long long * class_fp32(simint_b200_basis * b, size_t k)
+{
+    return (unsigned long long *)((char *)b->dqueue.ptr + k * SWEEP_QSTRIDE + sizeof(WorkQueue));
+}
+
+// Polls of about a microsecond a CTA waits on its launch's queue: every task
+// is published before the launch, so no wait happens in a sweep.
+#define SWEEP_SPIN_LIMIT 1000000ull
+
 // Issue the launches of class k (ERI chunks + checksums) on `stream`.
 static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout, long long cap,
                        cudaStream_t stream)
@@ -551,6 +636,7 @@ static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout,
     double * dsums = (double *)b->dsums.ptr;
     QClass & q = b->qcs[k];
     const long long chunk = full ? q.ntask : std::max<long long>(1, cap / q.nout);
+    const bool queued = class_uses_queue(q.req, 0, prec);
     for(long long t0 = 0; t0 < q.ntask; t0 += chunk)
     {
         const long long cn = std::min(chunk, q.ntask - t0);
@@ -560,6 +646,19 @@ static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout,
         a.task0 = t0;
         a.out = full ? dout + q.offset + t0 * q.nout : dout;
         a.gate = gate();
+        a.fp32_count = class_fp32(b, k);
+        if(queued)
+        {
+            // CTA-per-quartet kernels take their shell quartets from the
+            // class's work queue, heaviest first when the launch covers the
+            // whole class
+            a.wq = class_queue(b, k);
+            k_queue_reset<<<1, 1, 0, stream>>>(a.wq, cn, SWEEP_SPIN_LIMIT);
+            count_launch(1);
+            nl++;
+            if(q.has_perm && cn == q.ntask)
+                a.tperm = (const int *)((const char *)q.dev.ptr + perm_offset(q));
+        }
         int rc = launch_class(a, q.req, 0, 2, prec, stream);
         if(rc != 0)
             return rc;
@@ -580,6 +679,7 @@ static int issue_sweep(simint_b200_basis * b, int prec, double * dout, long long
 {
     int nl = 0;
     cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    cudaMemsetAsync(b->dqueue.ptr, 0, SWEEP_QSTRIDE * b->qcs.size(), stream);
     if(!events && cap >= b->total_out)
     {
         // full layout: classes write disjoint output ranges, so they run on
@@ -679,6 +779,13 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
             if(prec == SIMINT_B200_PREC_MIXED)
                 cand.push_back(VAR_WARP64);
         }
+        for(int v : {81, 82})
+            if(col_supported(q.req, 0, v))
+            {
+                cand.push_back(v);
+                if(prec == SIMINT_B200_PREC_MIXED)
+                    cand.push_back(v + 100);
+            }
         for(int v : {21, 22, 24, 28, 41, 42, 44, 48, 61, 62, 64, 68})
             if(coop2_supported(q.req, 0, v))
             {
@@ -815,12 +922,97 @@ extern "C" int simint_b200_basis_compute(simint_b200_basis * b, int prec, double
     return nl;
 }
 
+// Status words of the classes' work queues: SIMINT_B200_ERR_TIMEOUT when a
+// wait of the last sweep ran out.
+static int queue_status(simint_b200_basis * b)
+{
+    std::vector<char> h(SWEEP_QSTRIDE * b->qcs.size());
+    if(h.empty())
+        return 0;
+    if(cudaMemcpy(h.data(), b->dqueue.ptr, h.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        WorkQueue w;
+        memcpy(&w, h.data() + k * SWEEP_QSTRIDE, sizeof(w));
+        if(w.status)
+        {
+            set_error("a work-queue wait ran out");
+            return SIMINT_B200_ERR_TIMEOUT;
+        }
+    }
+    return 0;
+}
+
 extern "C" int simint_b200_basis_checksums(simint_b200_basis * b, double * sums)
 {
+    if(!b || !sums)
+        return SIMINT_B200_ERR_ARG;
     cudaDeviceSynchronize();
     if(cudaMemcpy(sums, b->dsums.ptr, 2 * sizeof(double) * b->qcs.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
         return SIMINT_B200_ERR_CUDA;
+    return queue_status(b);
+}
+
+extern "C" int simint_b200_basis_fp32_counts(simint_b200_basis * b, long long * counts)
+{
+    if(!b || !counts)
+        return SIMINT_B200_ERR_ARG;
+    cudaDeviceSynchronize();
+    std::vector<char> h(SWEEP_QSTRIDE * b->qcs.size());
+    if(!h.empty() && cudaMemcpy(h.data(), b->dqueue.ptr, h.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        unsigned long long c = 0;
+        memcpy(&c, h.data() + k * SWEEP_QSTRIDE + sizeof(WorkQueue), sizeof(c));
+        counts[k] = (long long)c;
+    }
     return 0;
+}
+
+extern "C" int simint_b200_basis_queue_probe(simint_b200_basis * b, int k, long long published, int closed,
+                                             int wait_ms, double * dev_out, long long dev_out_doubles)
+{
+    if(!b || k < 0 || k >= (int)b->qcs.size() || !dev_out || published < 0 || wait_ms < 0)
+        return SIMINT_B200_ERR_ARG;
+    QClass & q = b->qcs[k];
+    if(dev_out_doubles < q.ntask * q.nout || published > q.ntask)
+        return SIMINT_B200_ERR_ARG;
+    if(!class_uses_queue(q.req, 0, SIMINT_B200_PREC_FP64))
+    {
+        set_error("the class's kernel does not take work from a queue");
+        return SIMINT_B200_ERR_ARG;
+    }
+    Workspace & w = workspace();
+    if(!w.stream)
+        cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking);
+    KernArgs a;
+    fill_args(b, q, a);
+    a.ntask = q.ntask;
+    a.task0 = 0;
+    a.out = dev_out;
+    a.wq = class_queue(b, (size_t)k);
+    k_queue_set<<<1, 1, 0, w.stream>>>(a.wq, published, closed, 1000ull * (unsigned long long)wait_ms);
+    count_launch(1);
+    int rc = launch_class(a, q.req, 0, 2, SIMINT_B200_PREC_FP64, w.stream);
+    if(rc != 0)
+        return rc;
+    const cudaError_t e = cudaStreamSynchronize(w.stream);
+    if(e != cudaSuccess)
+    {
+        set_error(std::string("queue probe: ") + cudaGetErrorString(e));
+        return SIMINT_B200_ERR_CUDA;
+    }
+    WorkQueue hq;
+    if(cudaMemcpy(&hq, a.wq, sizeof(hq), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SIMINT_B200_ERR_CUDA;
+    if(hq.status)
+    {
+        set_error("a work-queue wait ran out");
+        return SIMINT_B200_ERR_TIMEOUT;
+    }
+    return (int)std::min<long long>(published, 0x7fffffff);
 }
 
 extern "C" int simint_b200_basis_class_times(simint_b200_basis * b, int prec, double * dev_out,

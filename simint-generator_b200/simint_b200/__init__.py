@@ -163,6 +163,7 @@ VAR_WARP, VAR_WARP64 = 6, 7                 # register kernel, one warp per shel
 VAR_COOP2 = {1: 21, 2: 22, 4: 24, 8: 28}          # cooperative kernel, 256 threads, batch B
 VAR_COOP2_128 = {1: 41, 2: 42, 4: 44, 8: 48}      # cooperative kernel, 128 threads, batch B
 VAR_COOP2_64 = {1: 61, 2: 62, 4: 64, 8: 68}       # cooperative kernel, 64 threads, batch B
+VAR_COL = {4: 81, 8: 82}                          # column kernel, NP primitive quartets per batch
 
 
 def get_variant(am, deriv=0, prec=0, lib=None):
@@ -315,10 +316,35 @@ class Basis:
         return self.lib.simint_b200_variant((C.c_int * 4)(*am), deriv, prec)
 
     def checksums(self):
+        """(nclass, 2): sum and sum of absolute values per class of the last
+        compute; raises when a work-queue wait of the sweep ran out."""
         n = self.lib.simint_b200_basis_nclass(self.h)
         s = np.zeros(2 * max(n, 1))
-        self.lib.simint_b200_basis_checksums(self.h, s.ctypes.data_as(_dp))
+        r = self.lib.simint_b200_basis_checksums(self.h, s.ctypes.data_as(_dp))
+        if r != 0:
+            raise RuntimeError("simint_b200_basis_checksums failed (%d): %s" % (r, last_error()))
         return s[:2 * n].reshape(n, 2)
+
+    def fp32_counts(self):
+        """Primitive quartets of the last compute that ran their VRR in FP32,
+        per class (int64 array)."""
+        n = self.lib.simint_b200_basis_nclass(self.h)
+        c = np.zeros(max(n, 1), dtype=np.int64)
+        self.lib.simint_b200_basis_fp32_counts.argtypes = [C.c_void_p, C.c_void_p]
+        r = self.lib.simint_b200_basis_fp32_counts(self.h, C.c_void_p(c.ctypes.data))
+        if r != 0:
+            raise RuntimeError("simint_b200_basis_fp32_counts failed: " + last_error())
+        return c[:n]
+
+    def queue_probe(self, k, published, closed, wait_ms, dev_ptr, ndoubles):
+        """simint_b200_basis_queue_probe: class k with a queue of `published`
+        tasks, closed or open; returns the C status (published, or
+        SIMINT_B200_ERR_TIMEOUT when a wait ran out)."""
+        L = self.lib
+        L.simint_b200_basis_queue_probe.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_int, C.c_int,
+                                                    C.c_void_p, C.c_longlong]
+        return L.simint_b200_basis_queue_probe(self.h, k, published, int(closed), wait_ms,
+                                               C.c_void_p(dev_ptr), ndoubles)
 
     @property
     def nbf(self):

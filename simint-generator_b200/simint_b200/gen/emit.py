@@ -110,6 +110,8 @@ def emit_class(am, prec="f64", warp=False):
         w("    }")
     for k in range(ntop):
         w("    double acc%d = 0.0;" % k)
+    if mixed:
+        w("    unsigned nlow = 0;            // primitive quartets run in FP32")
     if warp:
         w("    const int lane = threadIdx.x & 31;")
         w("    const int nj = c.kj1 - c.kj0, ncand = (c.bi1 - c.bi0) * nj;")
@@ -212,6 +214,7 @@ def emit_class(am, prec="f64", warp=False):
         w("            if(MIXED_GATE && s.lowprec)")
         w("            {")
         w("            s.make_f32();")
+        w("            nlow++;")
         o.extend(emit_vrr("float", "fmaf", "_f"))
         w("            }")
         w("            else")
@@ -220,6 +223,15 @@ def emit_class(am, prec="f64", warp=False):
         w("            }")
     w("        }")
     w("    }")
+    if mixed:
+        # FP32 primitive quartets of the converged threads, one atomic each
+        w("    if(MIXED_GATE && c.fp32_count)")
+        w("    {")
+        w("        const unsigned m = __activemask();")
+        w("        const unsigned tot = __reduce_add_sync(m, nlow);")
+        w("        if((int)(threadIdx.x & 31) == __ffs(m) - 1 && tot)")
+        w("            atomicAdd(c.fp32_count, (unsigned long long)tot);")
+        w("    }")
     if warp:
         # butterfly sums over the warp (every lane ends with the totals)
         w("    #pragma unroll")

@@ -12,6 +12,7 @@ import os
 
 from .emit import emit_class, unique_class, cname
 from .plan import class_plan
+from . import colgen
 
 HEADER = '#include "../ostei_device.cuh"\n#include "../kernels.h"\n\n'
 
@@ -76,6 +77,42 @@ def kernel_file(am):
     return "\n".join(o) + "\n"
 
 
+def _write(path, text):
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as f:
+            f.write(text)
+
+
+def col_classes(max_am):
+    """Unique classes that get a column kernel (colkern.cuh): the column
+    kernel's range with L >= 4 (below that the straight-line kernels win)."""
+    return [am for am in unique_classes(max_am) if colgen.col_supported(am) and sum(am) >= 4]
+
+
+def generate_col(outdir, max_am=4, only=None):
+    classes = col_classes(max_am)
+    if only is not None:
+        classes = [am for am in classes if am in only]
+    files = []
+    for am in classes:
+        path = os.path.join(outdir, "col_%s.cu" % cname(am))
+        _write(path, colgen.col_file(am))
+        files.append(path)
+    reg = ['#include "../colkern.cuh"', ""]
+    for am in classes:
+        reg.append("void register_col_%s(ColTable & t);" % cname(am))
+    reg.append("")
+    reg.append("void simint_b200_register_col(ColTable & t)")
+    reg.append("{")
+    for am in classes:
+        reg.append("    register_col_%s(t);" % cname(am))
+    reg.append("}")
+    path = os.path.join(outdir, "col_registry.cu")
+    _write(path, "\n".join(reg) + "\n")
+    files.append(path)
+    return files, classes
+
+
 def generate(outdir, max_am=4, limit=1300, only=None):
     os.makedirs(outdir, exist_ok=True)
     classes = [am for am in unique_classes(max_am) if straight_line_ok(am, limit)]
@@ -104,4 +141,5 @@ def generate(outdir, max_am=4, limit=1300, only=None):
         with open(path, "w") as f:
             f.write(text)
     files.append(path)
-    return files, classes
+    cfiles, _ = generate_col(outdir, max_am=max_am, only=only)
+    return files + cfiles, classes

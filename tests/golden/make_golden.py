@@ -15,7 +15,7 @@ shells normalised with the reference's simint_normalize_shells.
 Outputs (numpy .npz, a few hundred kB in total):
   valeev_deriv0.npz  every class up to (dd|dd), Psi4 order
   valeev_deriv1.npz  every class up to (pp|pp) and a set of d classes
-  valeev_fg.npz      f and g classes (deriv 0) with 1-6 primitives, exponents
+  valeev_fg.npz      f and g classes (deriv 0) with 1-3 primitives, exponents
                      in [0.05, 5e4] (the benchmark configurations' range) and
                      centres in a 6 bohr box; ValeevRef in Psi4 order
   valeev_fg_d1.npz   f classes, deriv 1, the same ranges
@@ -202,13 +202,27 @@ FG_D0 = [(3, 0, 0, 0), (3, 0, 3, 0), (3, 1, 3, 0), (3, 2, 1, 1), (3, 2, 2, 1), (
 FG_D1 = [(3, 0, 0, 0), (3, 1, 1, 0), (3, 2, 1, 1), (3, 1, 2, 2), (2, 2, 3, 0)]
 
 
-def make_fg(ref):
-    np.savez_compressed(os.path.join(HERE, "valeev_fg.npz"),
-                        **make_valeev(ref, 0, FG_D0, (1, 1, 1, 2), (1, 4), 13,
-                                      alpha=(0.05, 5e4), box=6.0))
-    np.savez_compressed(os.path.join(HERE, "valeev_fg_d1.npz"),
-                        **make_valeev(ref, 1, FG_D1, (1, 1, 1, 1), (1, 3), 14,
-                                      alpha=(0.05, 5e4), box=6.0))
+def _fg_one(job):
+    """One f/g class in a worker process (its own reference library handle
+    and a seed of its own, so the result does not depend on the order)."""
+    deriv, am, nsh, nprim, seed = job
+    ref = load_ref()
+    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=6.0)
+
+
+def make_fg(ref, workers=None):
+    """valeev_fg.npz / valeev_fg_d1.npz: one class per process (ValeevRef in
+    long double takes minutes for the largest of them)."""
+    import multiprocessing as mp
+    jobs0 = [(0, am, (1, 1, 1, 1), (1, 3), 1300 + k) for k, am in enumerate(FG_D0)]
+    jobs1 = [(1, am, (1, 1, 1, 1), (1, 3), 1400 + k) for k, am in enumerate(FG_D1)]
+    with mp.get_context("fork").Pool(workers or os.cpu_count()) as pool:
+        res = pool.map(_fg_one, jobs0 + jobs1, chunksize=1)
+    d0, d1 = {}, {}
+    for job, r in zip(jobs0 + jobs1, res):
+        (d1 if job[0] else d0).update(r)
+    np.savez_compressed(os.path.join(HERE, "valeev_fg.npz"), **d0)
+    np.savez_compressed(os.path.join(HERE, "valeev_fg_d1.npz"), **d1)
 
 
 if __name__ == "__main__":

@@ -75,3 +75,32 @@ def test_set_variant_validates_without_a_device():
     assert sb.set_variant((1, 1, 1, 1), 1, 1, sb.FP64, lib) != 0   # register kernels: deriv 0 only
     assert sb.set_variant(am, 0, 0, sb.FP64, lib) == 0
     assert sb.get_variant(am, 0, sb.FP64, lib) == 0
+
+
+def test_ctypes_struct_layouts_match_the_headers(tmp_path):
+    """The ctypes mirrors (simint_b200/capi.py) that the tests, the bench and
+    the Python bindings use have the layout of include/simint/shell/shell.h:
+    sizeof and every field's offsetof, from a C program built here."""
+    from simint_b200.capi import SimintShell, SimintMultiShellpair
+    structs = {"simint_shell": SimintShell, "simint_multi_shellpair": SimintMultiShellpair}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "simint/simint.h"', "int main(void){"]
+    for cname, py in structs.items():
+        lines.append('printf("%%s sizeof %%zu\\n", "%s", sizeof(struct %s));' % (cname, cname))
+        for f, _ in py._fields_:
+            lines.append('printf("%%s %%s %%zu\\n", "%s", "%s", offsetof(struct %s, %s));'
+                         % (cname, f, cname, f))
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    r = subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines():
+        a, b, c = line.split()
+        got[(a, b)] = int(c)
+    for cname, py in structs.items():
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

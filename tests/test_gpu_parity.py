@@ -109,3 +109,49 @@ def test_many_bra_pairs_padding(libs):
     assert r == rr == 27 * 6
     bad, dmax = parity_bad(out, ref)
     assert len(bad) == 0, dmax
+
+
+def test_ssss_clipped_ket_vector(libs):
+    """(ss|ss) with a ket list clipped inside a vector: the reference's
+    (ss|ss) kernel tests that vector with zeros past the clip
+    (skel/ostei_s_s_s_s.c), so a vector whose only large screening values
+    lie past the clip is skipped.  Ket pairs 0..4 tiny, 5..19 normal; clips
+    5 (vector skipped: zeros), 7 and 20 (computed); the caller's pair data
+    is left unchanged (the clip-20 call after the clip-5 one agrees with
+    the oracle too)."""
+    lib, orc = libs
+    rng = np.random.default_rng(606)
+    shells = [(0, tuple(rng.uniform(-1, 1, 3)), np.array([1.3]), np.array([0.8])),
+              (0, tuple(rng.uniform(-1, 1, 3)), np.array([0.7]), np.array([0.9]))]
+    for k in range(20):
+        c = 1e-10 if k < 5 else 0.7
+        for _ in range(2):
+            shells.append((0, tuple(rng.uniform(-2, 2, 3)), np.array([rng.uniform(0.3, 3.0)]), np.array([c])))
+    bra = [(0, 1)]
+    ket = [(2 + 2 * k, 3 + 2 * k) for k in range(20)]
+    S = ShellSet(shells)
+    tol = 1e-6
+    P = sb.make_pairs(lib, S, bra, 1)
+    Q = sb.make_pairs(lib, S, ket, 1)
+    oP = oracle_pairs(orc, S, bra, 1)
+    oQ = oracle_pairs(orc, S, ket, 1)
+    screen0 = np.ctypeslib.as_array(Q.screen, shape=(24,)).copy()
+    try:
+        for clip in (5, 20, 7, 5):
+            Q.nshell12_clip = clip
+            oQ.nshell12_clip = clip
+            r, out = sb.compute_eri(P, Q, tol, 0, lib)
+            rr, ref = oracle_eri(orc, oP, oQ, tol)
+            assert r == rr == clip
+            bad, dmax = parity_bad(out, ref)
+            assert len(bad) == 0, (clip, dmax)
+            if clip == 5:
+                assert (out == 0).all()
+            else:
+                assert np.abs(out[5:]).max() > 1e-3
+            assert np.array_equal(np.ctypeslib.as_array(Q.screen, shape=(24,)), screen0)
+    finally:
+        lib.simint_free_multi_shellpair(C.byref(P))
+        lib.simint_free_multi_shellpair(C.byref(Q))
+        orc.oracle_free_pair(C.byref(oP))
+        orc.oracle_free_pair(C.byref(oQ))

@@ -194,3 +194,64 @@ def test_oracle_matches_reflib_fg(am):
     bad, nover = quartets_unexplained(calc, ref, lambda q: ld(bras[q // len(kets)], kets[q % len(kets)]),
                                       int(np.prod([NC(a) for a in (am[0], am[1], am[2], am[3])])))
     assert not bad, (am, bad[:3])
+
+
+def _ssss_clip_case():
+    """s shells for a (ss|ss) call whose ket list is clipped inside a
+    vector: ket pairs 0..4 tiny (coefficients 1e-10), pairs 5..19 of normal
+    size, one primitive each, so the vector [0, 8) holds the five pairs below
+    the clip and three above it."""
+    rng = np.random.default_rng(606)
+    shells = [(0, tuple(rng.uniform(-1, 1, 3)), np.array([1.3]), np.array([0.8])),
+              (0, tuple(rng.uniform(-1, 1, 3)), np.array([0.7]), np.array([0.9]))]
+    for k in range(20):
+        c = 1e-10 if k < 5 else 0.7
+        shells.append((0, tuple(rng.uniform(-2, 2, 3)), np.array([rng.uniform(0.3, 3.0)]), np.array([c])))
+        shells.append((0, tuple(rng.uniform(-2, 2, 3)), np.array([rng.uniform(0.3, 3.0)]), np.array([c])))
+    bra = [(0, 1)]
+    ket = [(2 + 2 * k, 3 + 2 * k) for k in range(20)]
+    return shells, bra, ket
+
+
+def test_ssss_clipped_ket_vector():
+    """The reference's (ss|ss) kernel tests the vector at a clipped ket list's
+    end with zeros past the clip (skel/ostei_s_s_s_s.c) and writes those zeros
+    into the caller's pair data.  Pinned here: the reference run through the
+    driver (which keeps the pair data as created), repeated and after a
+    shorter clip, equals a fresh run; the last vector below the clip is
+    skipped (its pairs give zeros); our oracle follows the same rule."""
+    R = need("psi4_l4")
+    orc = load_oracle()
+    shells, bra, ket = _ssss_clip_case()
+    tol = 1e-6
+    R.set_shells(shells, normalize=False)
+
+    def ref_rows(clips):
+        kh = R.pairset(ket, 1)
+        bh = R.pairsets_single(bra, 1, 1)
+        outs = []
+        for c in clips:
+            o = np.zeros(c)
+            R.rows(bh, [kh], [c], 0, tol, 1, out=o, off=[0], count=False)
+            outs.append(o)
+        R.free_pairsets()
+        return outs
+
+    a5, a20, b5 = ref_rows([5, 20, 5])
+    (f20,) = ref_rows([20])
+    assert np.array_equal(a20, f20)          # the clip-5 call left no trace
+    assert np.array_equal(a5, b5)
+    assert (a5 == 0).all()                    # its only vector: skipped
+    assert np.abs(f20[5:]).max() > 1e-3
+
+    S = ShellSet(shells)
+    oP = oracle_pairs(orc, S, bra, 1)
+    oQ = oracle_pairs(orc, S, ket, 1)
+    for c, ref in ((5, a5), (20, f20)):
+        oQ.nshell12_clip = c
+        r, calc = oracle_eri(orc, oP, oQ, tol)
+        assert r == c
+        bad, dmax = parity_bad(calc, ref)
+        assert len(bad) == 0, (c, dmax)
+    orc.oracle_free_pair(C.byref(oP))
+    orc.oracle_free_pair(C.byref(oQ))

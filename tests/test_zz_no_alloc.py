@@ -20,7 +20,8 @@ import pytest
 import simint_b200 as sb
 from simint_b200.capi import ShellSet, PairP
 from simint_b200.workloads import random_shells
-from _util import parity_bad
+from oracle import load_oracle
+from _util import oracle_pairs, oracle_eri, parity_bad
 
 pytestmark = pytest.mark.gpu
 
@@ -64,6 +65,15 @@ def test_noalloc_matches_compute_eri(am, deriv, screen, tol):
     Q = sb.make_pairs(lib, S, ket, screen)
     r0, want = sb.compute_eri(P, Q, tol, deriv, lib)
     assert r0 == len(bra) * len(ket)
+    # the ordinary entry point against the CPU oracle on the same pairs
+    orc = load_oracle()
+    oP, oQ = oracle_pairs(orc, S, bra, screen), oracle_pairs(orc, S, ket, screen)
+    rr, ref = oracle_eri(orc, oP, oQ, tol, deriv, 0)
+    orc.oracle_free_pair(C.byref(oP))
+    orc.oracle_free_pair(C.byref(oQ))
+    assert rr == r0
+    bad, dmax = parity_bad(want, ref)
+    assert len(bad) == 0, dmax
     dP, dQ = _to_device(torch, lib, P), _to_device(torch, lib, Q)
     for call in range(2):
         out = torch.full((want.size,), float("nan"), dtype=torch.float64, device="cuda")
@@ -78,3 +88,37 @@ def test_noalloc_matches_compute_eri(am, deriv, screen, tol):
         assert len(bad) == 0, (call, dmax)
     lib.simint_free_multi_shellpair(C.byref(P))
     lib.simint_free_multi_shellpair(C.byref(Q))
+
+
+def test_noalloc_rejects_null_and_unsupported():
+    """NULL pair data is SIMINT_B200_ERR_ARG; a class whose shared-memory plan
+    exceeds the first cooperative kernel's limit ((gg|gg)) is
+    SIMINT_B200_ERR_CLASS, with real device buffers and nothing launched."""
+    torch = pytest.importorskip("torch")
+    lib = sb.load()
+    lib.simint_init()
+    _bind(lib)
+    assert lib.simint_b200_packed_size(None) == 0
+    rng = np.random.default_rng(5)
+    S = ShellSet(random_shells(rng, [4, 4, 4, 4], nprim_range=(1, 2), alpha=(0.3, 5.0), box=3.0))
+    lib.simint_normalize_shells(S.n, S.ptr(0))
+    P = sb.make_pairs(lib, S, [(0, 1)], 0)
+    Q = sb.make_pairs(lib, S, [(2, 3)], 0)
+    try:
+        dP, dQ = _to_device(torch, lib, P), _to_device(torch, lib, Q)
+        out = torch.zeros(15 ** 4, dtype=torch.float64, device="cuda")
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        r = lib.simint_b200_compute_eri_noalloc(0, None, C.c_void_p(dP.data_ptr()), C.byref(Q),
+                                                C.c_void_p(dQ.data_ptr()), 0.0, C.c_void_p(out.data_ptr()),
+                                                stream)
+        assert r == -5
+        r = lib.simint_b200_compute_eri_noalloc(0, C.byref(P), C.c_void_p(dP.data_ptr()), C.byref(Q),
+                                                C.c_void_p(dQ.data_ptr()), 0.0, C.c_void_p(out.data_ptr()),
+                                                stream)
+        assert r == -3
+        torch.cuda.synchronize()
+        host = np.zeros(8)
+        assert lib.simint_b200_pack(None, host.ctypes.data, host.nbytes) == -5
+    finally:
+        lib.simint_free_multi_shellpair(C.byref(P))
+        lib.simint_free_multi_shellpair(C.byref(Q))
