@@ -81,6 +81,9 @@ struct KernArgs
     // partial last vector below the clip, whose vector test covers only
     // them (empty range: no such vector)
     int kvec0, kvec1;
+    // MODE 2 (ss|ss): per bra pair, the end of its row's ket primitives
+    // (the clip of that row's ket list); nullptr: none
+    const int * kvend;
 };
 
 // The next queue slot of the calling thread's CTA (thread 0 calls it), or -1
@@ -408,6 +411,15 @@ __device__ __forceinline__ void make_ctx(const KernArgs & a, int iP, int iQ, Qua
     c.boys = a.boys;
     c.kvec0 = a.kvec0;
     c.kvec1 = a.kvec1;
+    if(a.kvend)
+    {
+        const int je = __ldg(a.kvend + iP);
+        if(je & 7)
+        {
+            c.kvec0 = je & ~7;
+            c.kvec1 = je;
+        }
+    }
     c.fp32_count = a.fp32_count;
 }
 

@@ -81,6 +81,7 @@ void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, do
 int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
                  cudaStream_t stream);
 bool class_uses_queue(const int req[4], int deriv, int prec);
+void permute_multi_shellpair(const simint_multi_shellpair * src, const int * order, simint_multi_shellpair * dst);
 void ssss_clip_vector(const simint_multi_shellpair * P, const simint_multi_shellpair * Q, int & v0, int & v1);
 
 // Generic (table-driven, dense) kernel for classes without a straight-line

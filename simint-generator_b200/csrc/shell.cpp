@@ -481,6 +481,70 @@ void simint_cat_multi_shellpair(int nmpair, struct simint_multi_shellpair const 
     Pout->nshell12_clip = nshell12;
 }
 
+} // extern "C"
+
+namespace sb200 {
+// dst = the shell pairs of src in the order order[0..nshell12), laid out as
+// simint_create_multi_shellpair would lay them out for that pair list (the
+// same padding rule, the same per-pair primitive order and values).
+void permute_multi_shellpair(const simint_multi_shellpair * src, const int * order, simint_multi_shellpair * dst)
+{
+    const int n = src->nshell12;
+    const int screen_method = src->screen ? SIMINT_SCREEN_SCHWARZ : 0;
+    std::vector<int> start(n > 0 ? n : 1);
+    int idx = 0;
+    for(int p = 0; p < n; p++)
+    {
+        start[p] = idx;
+        idx += src->nprim12[p];
+        if(((p + 1) % SIMINT_NSHELL_SIMD) == 0 || p + 1 >= n)
+            idx = SIMINT_SIMD_ROUND(idx);
+    }
+    int nprim = 0, batch = 0;
+    for(int s = 0; s < n; s++)
+    {
+        batch += src->nprim12[order[s]];
+        if(((s + 1) % SIMINT_NSHELL_SIMD) == 0 || s + 1 >= n)
+        {
+            nprim += SIMINT_SIMD_ROUND(batch);
+            batch = 0;
+        }
+    }
+    allocate_base(n, nprim, dst, screen_method);
+    dst->am1 = src->am1;
+    dst->am2 = src->am2;
+    dst->nprim = src->nprim;
+    dst->nshell12 = n;
+    dst->nshell12_clip = n;
+    dst->screen_max = src->screen_max;
+    idx = 0;
+    for(int s = 0; s < n; s++)
+    {
+        const int p = order[s];
+        for(int k = start[p]; k < start[p] + src->nprim12[p]; k++, idx++)
+        {
+            dst->x[idx] = src->x[k]; dst->y[idx] = src->y[k]; dst->z[idx] = src->z[k];
+            dst->PA_x[idx] = src->PA_x[k]; dst->PA_y[idx] = src->PA_y[k]; dst->PA_z[idx] = src->PA_z[k];
+            dst->PB_x[idx] = src->PB_x[k]; dst->PB_y[idx] = src->PB_y[k]; dst->PB_z[idx] = src->PB_z[k];
+            dst->alpha[idx] = src->alpha[k];
+            dst->prefac[idx] = src->prefac[k];
+            dst->alpha2[idx] = src->alpha2[k];
+            dst->beta2[idx] = src->beta2[k];
+            if(screen_method)
+                dst->screen[idx] = src->screen[k];
+        }
+        dst->AB_x[s] = src->AB_x[p];
+        dst->AB_y[s] = src->AB_y[p];
+        dst->AB_z[s] = src->AB_z[p];
+        dst->nprim12[s] = src->nprim12[p];
+        if(((s + 1) % SIMINT_NSHELL_SIMD) == 0 || s + 1 >= n)
+            pad_tail(dst, idx);
+    }
+}
+} // namespace sb200
+
+extern "C" {
+
 // shell.c:733-873: every input holds exactly one shell pair.
 void simint_cat_shellpairs(int nmpair, struct simint_multi_shellpair const ** Pin,
                            struct simint_multi_shellpair * Pout, int screen_method)

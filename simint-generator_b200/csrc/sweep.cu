@@ -56,7 +56,8 @@ struct QClass
     std::vector<long long> prefix;   // nb + 1
     std::vector<int> border;         // bra pair of each b
     bool has_perm = false;           // task order by primitive count uploaded
-    DevBuf dev;                      // prefix, border, task order
+    bool ssss = false;               // (ss|ss) with screening: per-row clipped-vector ends uploaded
+    DevBuf dev;                      // prefix, border, task order, (ss|ss) row ends
 };
 
 // Tasks of a class up to this count get a heaviest-first visiting order.
@@ -190,13 +191,22 @@ static size_t perm_offset(const QClass & q)
 // work queue -- tasks by decreasing primitive-pair product (a stable
 // counting sort), so the longest shell quartets start first and the short
 // ones fill the tail of the launch.
-static int upload_tasks(QClass & q, const PairClass & X, const PairClass & Y)
+static size_t kvend_offset(const QClass & q)
+{
+    return perm_offset(q) + (q.has_perm ? (((size_t)q.ntask * sizeof(int) + 255) & ~(size_t)255) : 0);
+}
+
+static int upload_tasks(QClass & q, const PairClass & X, const PairClass & Y, bool screened)
 {
     const size_t szp = (q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255;
     const size_t off = perm_offset(q);
     q.has_perm = q.ntask > 0 && q.ntask <= SWEEP_PERM_MAX;
     const size_t szperm = q.has_perm ? (size_t)q.ntask * sizeof(int) : 0;
-    if(!q.dev.reserve(off + szperm + 8))
+    // (ss|ss): the reference kernel's vector test at each row's clip (see
+    // ssss_clip_vector) needs the end of the row's ket primitives, per bra pair
+    q.ssss = screened && !q.req[0] && !q.req[1] && !q.req[2] && !q.req[3];
+    const size_t szkv = q.ssss ? (size_t)X.P.nshell12 * sizeof(int) : 0;
+    if(!q.dev.reserve(kvend_offset(q) + szkv + 8))
     {
         set_error("out of memory building task lists");
         return SIMINT_B200_ERR_CUDA;
@@ -228,6 +238,19 @@ static int upload_tasks(QClass & q, const PairClass & X, const PairClass & Y)
                 perm[(size_t)cnt[key(r, i)]++] = (int)t;
         cudaMemcpy((char *)q.dev.ptr + off, perm.data(), szperm, cudaMemcpyHostToDevice);
     }
+    if(q.ssss)
+    {
+        std::vector<int> ystart, kv((size_t)X.P.nshell12, 0);
+        int npad = 0;
+        pair_starts(&Y.P, ystart, npad);
+        for(size_t r = 0; r + 1 < q.prefix.size(); r++)
+        {
+            const long long n = q.prefix[r + 1] - q.prefix[r];
+            const int last = Y.order[(size_t)n - 1];
+            kv[(size_t)q.border[r]] = ystart[(size_t)last] + Y.P.nprim12[last];
+        }
+        cudaMemcpy((char *)q.dev.ptr + kvend_offset(q), kv.data(), szkv, cudaMemcpyHostToDevice);
+    }
     return 0;
 }
 
@@ -245,6 +268,7 @@ static void fill_args(const simint_b200_basis * b, const QClass & q, KernArgs & 
     a.border = (const int *)((const char *)q.dev.ptr + ((q.prefix.size() * sizeof(long long) + 255) & ~(size_t)255));
     a.korder = Y.dorder;
     a.nb = (int)q.border.size();
+    a.kvend = q.ssss ? (const int *)((const char *)q.dev.ptr + kvend_offset(q)) : nullptr;
 }
 
 extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simint_shell const * shells,
@@ -301,7 +325,7 @@ extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simin
         simint_create_multi_shellpair2(n, AB.data(), &pc.P,
                                        screen_tol > 0.0 ? SIMINT_SCREEN_SCHWARZ : SIMINT_SCREEN_NONE);
         PackedLayout L;
-        const size_t sz = (pack_pairs(&pc.P, nullptr, L) + 255) & ~(size_t)255;
+        size_t sz = (pack_pairs(&pc.P, nullptr, L) + 255) & ~(size_t)255;
         const size_t szo = ((size_t)n * sizeof(int) + 255) & ~(size_t)255;
         const size_t szq = (size_t)n * sizeof(double);
         if(!pc.dev.reserve(sz + szo + szq) || !w.hstage.reserve(sz))
@@ -327,6 +351,44 @@ extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simin
         pc.order.resize(n);
         std::iota(pc.order.begin(), pc.order.end(), 0);
         std::stable_sort(pc.order.begin(), pc.order.end(), [&](int x, int y) { return pc.Q[x] > pc.Q[y]; });
+        // Store the pairs in that order: a row's kets are then a prefix of
+        // the set, exactly the clipped sorted list a caller of
+        // simint_compute_eri passes, and the 8-wide vector screening groups
+        // the same primitives as it does for that caller.
+        bool sorted = true;
+        for(int k = 0; k < n && sorted; k++)
+            sorted = pc.order[k] == k;
+        if(!sorted)
+        {
+            simint_multi_shellpair S;
+            simint_initialize_multi_shellpair(&S);
+            permute_multi_shellpair(&pc.P, pc.order.data(), &S);
+            simint_free_multi_shellpair(&pc.P);
+            pc.P = S;
+            std::vector<int> sa(n), sbv(n);
+            std::vector<double> q(n);
+            for(int k = 0; k < n; k++)
+            {
+                sa[k] = pc.sa[pc.order[k]];
+                sbv[k] = pc.sb[pc.order[k]];
+                q[k] = pc.Q[pc.order[k]];
+            }
+            pc.sa.swap(sa);
+            pc.sb.swap(sbv);
+            pc.Q.swap(q);
+            std::iota(pc.order.begin(), pc.order.end(), 0);
+            const size_t sz2 = (pack_pairs(&pc.P, nullptr, L) + 255) & ~(size_t)255;
+            if(!pc.dev.reserve(sz2 + szo) || !w.hstage.reserve(sz2))
+            {
+                set_error("out of memory building the basis");
+                simint_b200_basis_free(b);
+                return nullptr;
+            }
+            pack_pairs(&pc.P, (char *)w.hstage.ptr, L);
+            cudaMemcpy(pc.dev.ptr, w.hstage.ptr, sz2, cudaMemcpyHostToDevice);
+            pc.view = device_view((const char *)pc.dev.ptr, L, pc.P.screen_max);
+            sz = sz2;
+        }
         cudaMemcpy((char *)pc.dev.ptr + sz, pc.order.data(), n * sizeof(int), cudaMemcpyHostToDevice);
         pc.dorder = (const int *)((char *)pc.dev.ptr + sz);
     }
@@ -377,7 +439,7 @@ extern "C" simint_b200_basis * simint_b200_basis_create(int nshell, struct simin
             q.nfull = tot;
             if(tot == 0)
                 continue;
-            if(upload_tasks(q, X, Y) != 0)
+            if(upload_tasks(q, X, Y, screen_tol > 0.0) != 0)
             {
                 simint_b200_basis_free(b);
                 return nullptr;
@@ -428,7 +490,7 @@ extern "C" int simint_b200_basis_subsample(simint_b200_basis * b, long long maxq
         q.border.swap(bor);
         q.ntask = q.prefix.back();
         q.nprimq = 0;
-        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky]) != 0)
+        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky], b->tol > 0.0) != 0)
             return SIMINT_B200_ERR_CUDA;
     }
     layout_outputs(b);
@@ -474,7 +536,7 @@ extern "C" int simint_b200_basis_subsample_stride(simint_b200_basis * b, int str
         q.border.swap(bor);
         q.ntask = q.prefix.back();
         q.nprimq = 0;
-        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky]) != 0)
+        if(upload_tasks(q, b->pcs[q.bx], b->pcs[q.ky], b->tol > 0.0) != 0)
             return SIMINT_B200_ERR_CUDA;
     }
     layout_outputs(b);

@@ -17,7 +17,7 @@ Outputs (numpy .npz, a few hundred kB in total):
   valeev_deriv1.npz  every class up to (pp|pp) and a set of d classes
   valeev_fg.npz      f and g classes (deriv 0) with 1-3 primitives, exponents
                      in [0.05, 5e4] (the benchmark configurations' range) and
-                     centres in a 6 bohr box; ValeevRef in Psi4 order
+                     centres in a 2.5 bohr box; ValeevRef in Psi4 order
   valeev_fg_d1.npz   f classes, deriv 1, the same ranges
   boys_ref.npz       reference boys_F_split values and grid rows
   pairs_ref.npz      reference multi-shell-pair arrays (no screening and
@@ -207,7 +207,7 @@ def _fg_one(job):
     and a seed of its own, so the result does not depend on the order)."""
     deriv, am, nsh, nprim, seed = job
     ref = load_ref()
-    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=6.0)
+    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=2.5)
 
 
 def make_fg(ref, workers=None):
@@ -221,8 +221,10 @@ def make_fg(ref, workers=None):
     d0, d1 = {}, {}
     for job, r in zip(jobs0 + jobs1, res):
         (d1 if job[0] else d0).update(r)
-    np.savez_compressed(os.path.join(HERE, "valeev_fg.npz"), **d0)
-    np.savez_compressed(os.path.join(HERE, "valeev_fg_d1.npz"), **d1)
+    for name, d in (("valeev_fg.npz", d0), ("valeev_fg_d1.npz", d1)):
+        tmp = os.path.join(HERE, "." + name + ".tmp.npz")
+        np.savez_compressed(tmp, **d)
+        os.replace(tmp, os.path.join(HERE, name))
 
 
 if __name__ == "__main__":
