@@ -124,6 +124,13 @@ int simint_b200_basis_quartet(simint_b200_basis const * b, int k, long long q, i
  * q < the class's quartet count (host array of 4 ints per quartet). */
 int simint_b200_basis_class_quartets(simint_b200_basis const * b, int k, int * shells);
 
+/* The ket pair list of class k in the order the sweep stores it (decreasing
+ * Schwarz bound Q_cd): shells[2i], shells[2i+1] of pair i when shells is
+ * not NULL.  Every row of the class takes a prefix of this list (a row is
+ * simint_compute_eri(bra pair, this list with nshell12_clip = the row's ket
+ * count)).  Returns the number of pairs or a negative code. */
+int simint_b200_basis_class_kets(simint_b200_basis const * b, int k, int * shells);
+
 /* Per-class checksums of the last compute: sums[2k] = sum of values,
  * sums[2k+1] = sum of absolute values.  Waits for the device.  Returns
  * SIMINT_B200_ERR_TIMEOUT when a bounded work-queue wait of the sweep ran

@@ -32,13 +32,15 @@ bool col_is_variant(int v) { return v >= 81 && v <= 80 + COL_NNP; }
 
 struct ColLayout
 {
-    int npi, nt, vdoubles;
+    int npi, nt, vdoubles, fs;
     size_t smem;
 };
 
-// Shared memory of a launch: the recursion area V (also the slot-sum and
-// HRR scratch), the coefficient records, the accumulators of the HRR and
-// the two survivor lists.
+// Shared memory of a launch: the recursion area V (the bra block of FS
+// primitive quartets and the stage areas of a batch of NP; also the
+// slot-sum and HRR scratch), the coefficient records of a block, the
+// accumulators of the HRR and the two survivor lists.  FS is the largest of
+// 32, 16, 8, 4 (a multiple of NP) that fits.
 static bool col_layout(const ColKernels & k, const C2Params & p, int v, ColLayout & L)
 {
     L.npi = v - 81;
@@ -46,13 +48,22 @@ static bool col_layout(const ColKernels & k, const C2Params & p, int v, ColLayou
         return false;
     const int np = COL_NPS[L.npi];
     L.nt = k.nt[L.npi];
-    int vd = std::max(k.vdoubles_per_np * np, k.red_per_np * np);
-    vd = std::max(vd, p.hrr_need);
-    L.vdoubles = (vd + 1) & ~1;
     const size_t acc = (size_t)((p.acc_size + 1) & ~1);
-    L.smem = ((size_t)L.vdoubles + (size_t)k.ncoef * k.ns[L.npi] + acc) * sizeof(double)
-           + 2 * (size_t)L.nt * sizeof(int);
-    return L.smem <= 220 * 1024;
+    for(int fs = 32; fs >= np; fs /= 2)
+    {
+        int vd = std::max(k.f0b * fs + k.sab * np, k.red_per_np * np);
+        vd = std::max(vd, p.hrr_need);
+        vd = (vd + 1) & ~1;
+        const size_t smem = ((size_t)vd + (size_t)k.ncoef * fs + acc) * sizeof(double) + 2 * (size_t)L.nt * sizeof(int);
+        if(smem <= 220 * 1024)
+        {
+            L.fs = fs;
+            L.vdoubles = vd;
+            L.smem = smem;
+            return true;
+        }
+    }
+    return false;
 }
 
 bool col_supported(const int req[4], int deriv, int v)
@@ -112,7 +123,7 @@ int launch_col(KernArgs & a, const int req[4], int mode, int prec, cudaStream_t 
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     long long grid = std::min<long long>(a.ntask, (long long)nsm * per_sm);
     grid = std::max<long long>(grid, 1);
-    fn<<<(unsigned)grid, L.nt, L.smem, stream>>>(a, p, L.vdoubles);
+    fn<<<(unsigned)grid, L.nt, L.smem, stream>>>(a, p, L.vdoubles, L.fs);
     count_launch(1);
     return 0;
 }

@@ -13,11 +13,14 @@
 //
 // Per shell quartet: the surviving primitive quartets (the reference's
 // primitive screening, in order; in mixed mode split into an FP64 and an FP32
-// list by the error gate) are set up 64 at a time (set-up and Boys, one
-// thread each, into shared memory: col_setup) and processed in batches of NP:
-//   1. the bra-only recursion (g_e, 0|0)^(m), level by level (col_f0),
-//   2. the ket stages f = 1..c+d (generated per class: CT::stages), the top
-//      quartets summed into per-thread FP64 registers;
+// list by the error gate) are processed in blocks of FS (up to 32, chosen per
+// class to fit shared memory):
+//   1. set-up and Boys, one thread per primitive quartet (col_setup),
+//   2. the bra-only recursion (g_e, 0|0)^(m) of the whole block, level by
+//      level, into a level-major block in shared memory (col_f0_block),
+//   3. per batch of NP primitive quartets of the block, the ket stages
+//      f = 1..c+d (generated per class: CT::stages), the top quartets summed
+//      into per-thread FP64 registers;
 // then the per-thread sums are added over the batch slots in a fixed order
 // into the cooperative kernel's accumulator layout, and its HRR
 // (c2_hrr_side, OSTEI_HRR_Algorithm_Base.cpp:160-283) runs in shared memory
@@ -35,14 +38,12 @@
 __device__ __forceinline__ double cfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float cfma(float a, float b, float c) { return fmaf(a, b, c); }
 
-// coefficient record of a set-up primitive quartet (doubles, rows of NS)
+// coefficient record of a set-up primitive quartet (doubles, rows of FS)
 enum { CC_XP = 0, CC_YP = 3, CC_XQ = 6, CC_YQ = 9, CC_ZP = 12, CC_ZQ = 13, CC_O2P = 14, CC_O2Q = 15,
        CC_O2PQ = 16, CC_F = 17 };
 
 __host__ __device__ constexpr int col_lo(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
 __host__ __device__ constexpr int col_nt(int nrole, int np) { return ((nrole * np + 31) / 32) * 32; }
-// survivors set up at once (one thread each)
-__host__ __device__ constexpr int col_ns(int nrole, int np) { return col_nt(nrole, np) < 64 ? col_nt(nrole, np) : 64; }
 
 // Cartesian exponents of flat index g (levels in order, Psi4 order inside a
 // level) and its level.
@@ -69,6 +70,16 @@ __device__ __forceinline__ int col_flat(int i, int j, int k)
     return col_lo(l) + ((l - i) * (l - i + 1)) / 2 + k;
 }
 
+// First row of level e in the level-major bra block: levels 0..e-1 hold
+// orders 0..L-e' of their nc(e') functions.
+__host__ __device__ constexpr int col_lb(int L, int e)
+{
+    int r = 0;
+    for(int x = 0; x < e; x++)
+        r += ((x + 1) * (x + 2)) / 2 * (L - x + 1);
+    return r;
+}
+
 __device__ __forceinline__ int col_stepdir(int i, int j, int k)
 {
     const int e[3] = {i, j, k};
@@ -80,16 +91,16 @@ __device__ __forceinline__ int col_stepdir(int i, int j, int k)
     return 0;
 }
 
-// Set-up and Boys values of survivors list[s0 .. s0 + NS) (NS threads in
+// Set-up and Boys values of survivors list[s0 .. s0 + FS) (FS threads in
 // parallel; slots past n get zeros, which run through the recursion as
-// zeros) into coef[k * NS + slot].
-template<class CT, int NS>
+// zeros) into coef[k * FS + slot].
+template<class CT>
 __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
                                           int nj, unsigned long long njinv, bool fastdiv,
-                                          double * __restrict__ coef)
+                                          double * __restrict__ coef, int FS)
 {
     const int tid = threadIdx.x;
-    if(tid < NS)
+    if(tid < FS)
     {
         const int g = s0 + tid;
         double v[CC_F + CT::L + 1];
@@ -114,122 +125,170 @@ __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __re
         }
         #pragma unroll
         for(int k = 0; k < CC_F + CT::L + 1; k++)
-            coef[k * NS + tid] = v[k];
+            coef[k * FS + tid] = v[k];
     }
     __syncthreads();
 }
 
-// Bra-only recursion of a batch: F0[(m * NROLE + g) * NP + slot] =
-// (g, 0 | 0)^(m) for every bra function g of levels 0..E, orders
-// 0..L - level (level 0: F_m times the pair prefactors).  Work items
-// (function, slot) of a level spread over the CTA; one barrier per level.
-template<typename T, class CT, int NP, int NT, int NS>
-__device__ __forceinline__ void col_f0(T * __restrict__ F0, const double * __restrict__ coef)
+// Bra-only recursion of a block of FS primitive quartets into the
+// level-major block F0: (g, 0|0)^(m) of bra function g = lo(e) + p at
+// F0[(lb(e) + m * nc(e) + p) * FS + slot], orders 0..L - e (level 0: F_m
+// times the pair prefactors).  Work items (function, slot) of a level spread
+// over the CTA; one barrier per level.
+template<typename T, class CT, int NT>
+__device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS)
 {
-    constexpr int RS = CT::NROLE * NP;
     const int tid = threadIdx.x;
-    if(tid < NP)
+    for(int it = tid; it < (CT::L + 1) * FS; it += NT)
     {
-        #pragma unroll
-        for(int m = 0; m <= CT::L; m++)
-            F0[m * RS + tid] = (T)coef[(CC_F + m) * NS + tid];
+        const int m = it / FS, slot = it - m * FS;
+        F0[m * FS + slot] = (T)coef[(CC_F + m) * FS + slot];
     }
     __syncthreads();
-    #pragma unroll
+    int lb2 = 0, lb1 = 0, lbe = CT::L + 1;           // first rows of levels e-2, e-1, e
+    #pragma unroll 1
     for(int e = 1; e <= CT::E; e++)
     {
-        const int nitem = ((e + 1) * (e + 2) / 2) * NP;
+        const int nce = ((e + 1) * (e + 2)) / 2, nc1 = (e * (e + 1)) / 2, nc2 = ((e - 1) * e) / 2;
+        const int nitem = nce * FS;
         for(int it = tid; it < nitem; it += NT)
         {
-            const int pe = it / NP, slot = it - pe * NP;
+            const int pe = it / FS, slot = it - pe * FS;
             int i, j, k, l;
             col_cart(col_lo(e) + pe, i, j, k, l);
             const int x = col_stepdir(i, j, k);
             int q[3] = {i, j, k};
             const int n = q[x] - 1;
             q[x] -= 1;
-            const int g1 = col_flat(q[0], q[1], q[2]);
+            const int p1 = col_flat(q[0], q[1], q[2]) - col_lo(e - 1);
             q[x] -= 1;
-            const int g2 = n > 0 ? col_flat(q[0], q[1], q[2]) : 0;
-            const T XP = (T)coef[(CC_XP + x) * NS + slot];
-            const T YP = (T)coef[(CC_YP + x) * NS + slot];
-            const T Zp = (T)coef[CC_ZP * NS + slot];
-            const T k2 = (T)((double)n * coef[CC_O2P * NS + slot]);
-            const T * s1 = F0 + g1 * NP + slot;
-            const T * s2 = F0 + g2 * NP + slot;
-            T * dst = F0 + (col_lo(e) + pe) * NP + slot;
-            #pragma unroll
+            const int p2 = n > 0 ? col_flat(q[0], q[1], q[2]) - col_lo(e - 2) : 0;
+            const T XP = (T)coef[(CC_XP + x) * FS + slot];
+            const T YP = (T)coef[(CC_YP + x) * FS + slot];
+            const T Zp = (T)coef[CC_ZP * FS + slot];
+            const T k2 = (T)((double)n * coef[CC_O2P * FS + slot]);
+            const T * s1 = F0 + (lb1 + p1) * FS + slot;
+            const T * s2 = F0 + (n > 0 ? (lb2 + p2) * FS + slot : 0);
+            T * dst = F0 + (lbe + pe) * FS + slot;
+            const int st1 = nc1 * FS, st2 = nc2 * FS, st = nce * FS;
             for(int m = 0; m <= CT::L - e; m++)
             {
-                T r = XP * s1[m * RS];
-                r = cfma(YP, s1[(m + 1) * RS], r);
+                T r = XP * s1[m * st1];
+                r = cfma(YP, s1[(m + 1) * st1], r);
                 if(n > 0)
-                    r = cfma(k2, cfma(Zp, s2[(m + 1) * RS], s2[m * RS]), r);
-                dst[m * RS] = r;
+                    r = cfma(k2, cfma(Zp, s2[(m + 1) * st2], s2[m * st2]), r);
+                dst[m * st] = r;
             }
         }
         __syncthreads();
+        lb2 = lb1;
+        lb1 = lbe;
+        lbe += nce * (CT::L - e + 1);
     }
 }
 
-// One batch of NP set-up survivors (coef: the first member's record, row
-// stride NS) in type T.
-template<typename T, class CT, int NP, int NT, int NS>
-__device__ __forceinline__ void col_batch(const double * __restrict__ coef, double * __restrict__ V,
-                                          int role, int slot, bool valid, const int (&loff)[3],
-                                          const int (&ny)[3], double (&acc)[CT::NTOP])
+// Per-thread constants of the column kernel: the thread's role (bra
+// function g_e) and slot, its positions in the batch areas (own, loff) and
+// in the bra block (ownF + m * ostr: order m of its own column; loffF[y] +
+// m * mstrF[y]: order m of g_e - 1_y).
+struct ColThread
 {
-    T * F0 = (T *)V;
-    T * SB = F0;                                            // stage 2, 4, ... (F0 is dead by then)
-    T * SA = F0 + (CT::F0N > CT::SBN ? CT::F0N : CT::SBN) * NP;
-    col_f0<T, CT, NP, NT, NS>(F0, coef);
+    int role, slot, own, ownF, ostr;
+    bool valid;
+    int ny[3], loff[3], loffF[3], mstrF[3];
+};
+
+template<class CT, int NP>
+__device__ __forceinline__ void col_thread(ColThread & t, int FS)
+{
+    const int tid = threadIdx.x;
+    t.role = tid / NP;
+    t.slot = tid - t.role * NP;
+    t.valid = t.role < CT::NROLE;
+    int ri = 0, rj = 0, rk = 0, re = 0;
+    if(t.valid)
+        col_cart(t.role, ri, rj, rk, re);
+    t.ny[0] = ri; t.ny[1] = rj; t.ny[2] = rk;
+    t.own = t.role * NP + t.slot;
+    const int pe = t.valid ? t.role - col_lo(re) : 0;
+    const int lbr = col_lb(CT::L, re), lbr1 = re > 0 ? col_lb(CT::L, re - 1) : 0;
+    t.ownF = t.valid ? (lbr + pe) * FS + t.slot : t.slot;
+    t.ostr = ((re + 1) * (re + 2)) / 2 * FS;
+    #pragma unroll
+    for(int y = 0; y < 3; y++)
+    {
+        int q[3] = {ri, rj, rk};
+        q[y] -= 1;
+        const bool has = t.valid && t.ny[y] > 0;
+        const int g1 = has ? col_flat(q[0], q[1], q[2]) : 0;
+        // absent g_e - 1_y: the thread's own position (its coefficient n_y
+        // is 0 and the value read is a finite one)
+        t.loff[y] = (has ? g1 : (t.valid ? t.role : 0)) * NP + t.slot;
+        t.loffF[y] = has ? (lbr1 + g1 - col_lo(re - 1)) * FS + t.slot : t.ownF;
+        t.mstrF[y] = has ? (re * (re + 1)) / 2 * FS : t.ostr;
+    }
+}
+
+// The ket stages of batch [b0, b0 + NP) of a block (coef: the block's
+// records, row stride FS) in type T.
+template<typename T, class CT, int NP>
+__device__ __forceinline__ void col_batch(const T * __restrict__ F0, T * __restrict__ SA, T * __restrict__ SB,
+                                          const double * __restrict__ coef, int FS, int b0,
+                                          const ColThread & t, double (&acc)[CT::NTOP])
+{
+    const int cs = b0 + t.slot;
     T XQ[3], YQ[3], cB[3], kq[CT::KQN], Zq = 0;
     #pragma unroll
     for(int y = 0; y < 3; y++)
     {
-        XQ[y] = valid ? (T)coef[(CC_XQ + y) * NS + slot] : (T)0;
-        YQ[y] = valid ? (T)coef[(CC_YQ + y) * NS + slot] : (T)0;
-        cB[y] = valid ? (T)((double)ny[y] * coef[CC_O2PQ * NS + slot]) : (T)0;
+        XQ[y] = t.valid ? (T)coef[(CC_XQ + y) * FS + cs] : (T)0;
+        YQ[y] = t.valid ? (T)coef[(CC_YQ + y) * FS + cs] : (T)0;
+        cB[y] = t.valid ? (T)((double)t.ny[y] * coef[CC_O2PQ * FS + cs]) : (T)0;
     }
-    if(valid)
-        Zq = (T)coef[CC_ZQ * NS + slot];
+    if(t.valid)
+        Zq = (T)coef[CC_ZQ * FS + cs];
     #pragma unroll
     for(int k = 0; k < CT::KQN; k++)
-        kq[k] = valid ? (T)((double)(k + 1) * coef[CC_O2Q * NS + slot]) : (T)0;
-    CT::template stages<T, NP>(F0, SA, SB, role * NP + slot, loff, XQ, YQ, Zq, kq, cB, valid, acc);
+        kq[k] = t.valid ? (T)((double)(k + 1) * coef[CC_O2Q * FS + cs]) : (T)0;
+    CT::template stages<T, NP>(F0 + b0, SA, SB, t.own, t.ownF, t.ostr, t.loff, t.loffF, t.mstrF, XQ, YQ, Zq, kq,
+                               cB, t.valid, acc);
+}
+
+// One block of survivors list[s0 ..) in type T: set-up, bra block, batches.
+template<typename T, class CT, int NP, int NT>
+__device__ __forceinline__ void col_block(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
+                                          int nj, unsigned long long njinv, bool fastdiv, double * __restrict__ coef,
+                                          double * __restrict__ V, int FS, const ColThread & t,
+                                          double (&acc)[CT::NTOP])
+{
+    T * F0 = (T *)V;
+    T * SA = F0 + CT::F0B * FS;
+    T * SB = SA + CT::SAN * NP;
+    col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS);
+    col_f0_block<T, CT, NT>(F0, coef, FS);
+    const int nb = min(FS, n - s0);
+    for(int b0 = 0; b0 < nb; b0 += NP)
+        col_batch<T, CT, NP>(F0, SA, SB, coef, FS, b0, t, acc);
 }
 
 template<class CT, int MODE, bool MIXED, int NP>
 __global__ void __launch_bounds__(col_nt(CT::NROLE, NP), 1)
-k_col(const KernArgs a, const C2Params p, const int vdoubles)
+k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
 {
     constexpr int NT = col_nt(CT::NROLE, NP);
-    constexpr int NS = col_ns(CT::NROLE, NP);
     extern __shared__ __align__(16) double sm[];
     __shared__ int wcount[2][NT / 32];
     __shared__ int s_cnt[2];
     __shared__ long long s_qslot;
     double * V = sm;
     double * coef = sm + vdoubles;
-    double * acc2 = coef + (CC_F + CT::L + 1) * NS;
+    double * acc2 = coef + (CC_F + CT::L + 1) * FS;
     int * surv = (int *)(acc2 + ((p.acc_size + 1) & ~1));   // [0, NT): FP64 list, [NT, 2 NT): FP32 list
     const int tid = threadIdx.x;
-    const int role = tid / NP, slot = tid - role * NP;
-    const bool valid = role < CT::NROLE;
-    int ri = 0, rj = 0, rk = 0, re = 0;
-    if(valid)
-        col_cart(role, ri, rj, rk, re);
-    const int ny[3] = {ri, rj, rk};
-    // shared-memory position of (g_e - 1_y) (own position when absent: its
-    // coefficient n_y(g_e) is then 0 and the value read is a finite one)
-    int loff[3];
-    #pragma unroll
-    for(int y = 0; y < 3; y++)
-    {
-        int q[3] = {ri, rj, rk};
-        q[y] -= 1;
-        loff[y] = (valid && ny[y] > 0 ? col_flat(q[0], q[1], q[2]) : (valid ? role : 0)) * NP + slot;
-    }
+    ColThread th;
+    col_thread<CT, NP>(th, FS);
+    const int role = th.role, slot = th.slot;
+    const bool valid = th.valid;
     const int lane = tid & 31, warp = tid >> 5;
     long long t = 0;
     for(long long qslot = blockIdx.x; cta_next_task(a, qslot, t, &s_qslot); qslot += gridDim.x)
@@ -309,20 +368,12 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles)
             const int nhi = s_cnt[0], nlo = s_cnt[1];
             if(MIXED && tid == 0 && nlo > 0 && a.fp32_count)
                 atomicAdd(a.fp32_count, (unsigned long long)nlo);
-            for(int s0 = 0; s0 < nhi; s0 += NS)
-            {
-                col_setup<CT, NS>(c, surv, s0, nhi, nj, njinv, fastdiv, coef);
-                for(int g0 = 0; g0 < NS && s0 + g0 < nhi; g0 += NP)
-                    col_batch<double, CT, NP, NT, NS>(coef + g0, V, role, slot, valid, loff, ny, acc);
-            }
+            for(int s0 = 0; s0 < nhi; s0 += FS)
+                col_block<double, CT, NP, NT>(c, surv, s0, nhi, nj, njinv, fastdiv, coef, V, FS, th, acc);
             if constexpr(MIXED)
             {
-                for(int s0 = 0; s0 < nlo; s0 += NS)
-                {
-                    col_setup<CT, NS>(c, surv + NT, s0, nlo, nj, njinv, fastdiv, coef);
-                    for(int g0 = 0; g0 < NS && s0 + g0 < nlo; g0 += NP)
-                        col_batch<float, CT, NP, NT, NS>(coef + g0, V, role, slot, valid, loff, ny, acc);
-                }
+                for(int s0 = 0; s0 < nlo; s0 += FS)
+                    col_block<float, CT, NP, NT>(c, surv + NT, s0, nlo, nj, njinv, fastdiv, coef, V, FS, th, acc);
             }
             __syncthreads();      // surv, s_cnt and wcount are reused
         }
@@ -377,7 +428,7 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles)
 // registry of the generated classes
 // ---------------------------------------------------------------------
 
-typedef void (*ColFn)(const KernArgs, const C2Params, const int);
+typedef void (*ColFn)(const KernArgs, const C2Params, const int, const int);
 
 #define COL_NNP 2
 static constexpr int COL_NPS[COL_NNP] = {4, 8};
@@ -386,11 +437,11 @@ struct ColKernels
 {
     int am[4];
     int L, nrole, ntop;
-    int vdoubles_per_np;                 // doubles of the F0|SA|SB region per batch slot
+    int f0b;                             // doubles of the bra block per slot
+    int sab;                             // doubles of the stage areas SA + SB per batch slot
     int red_per_np;                      // doubles of the slot-sum scratch per batch slot
     int ncoef;                           // doubles of a coefficient record
     int nt[COL_NNP];                     // threads per CTA for each NP
-    int ns[COL_NNP];                     // survivors set up at once for each NP
     ColFn fn[COL_NNP][3][2];             // [np][mode][fp64, mixed]
 };
 
@@ -405,7 +456,6 @@ static void col_fill_np(ColKernels & k)
 {
     constexpr int NP = COL_NPS[NPI];
     k.nt[NPI] = col_nt(CT::NROLE, NP);
-    k.ns[NPI] = col_ns(CT::NROLE, NP);
     for(int md = 0; md < 3; md++)
         k.fn[NPI][md][0] = k.fn[NPI][md][1] = nullptr;
     if constexpr(col_nt(CT::NROLE, NP) <= 1024)
@@ -425,7 +475,8 @@ static void col_fill(ColKernels & k)
     k.L = CT::L;
     k.nrole = CT::NROLE;
     k.ntop = CT::NTOP;
-    k.vdoubles_per_np = (CT::F0N > CT::SBN ? CT::F0N : CT::SBN) + CT::SAN;
+    k.f0b = CT::F0B;
+    k.sab = CT::SAN + CT::SBN;
     k.red_per_np = CT::NTOP * (CT::NROLE - col_lo(CT::A0));
     k.ncoef = CC_F + CT::L + 1;
     col_fill_np<CT, 0>(k);

@@ -381,6 +381,85 @@ size_t pack_pairs(const simint_multi_shellpair * P, char * dst, PackedLayout & L
     return total;
 }
 
+// Byte offsets of a pair set's arrays inside its allocation (-1: absent).
+struct SoaOffsets
+{
+    long long x, y, z, pax, pay, paz, pbx, pby, pbz, alpha, prefac, screen, a2, b2, abx, aby, abz, nprim12;
+};
+
+// The device records of pack_records, built from a device copy of the pair
+// set's arrays: one thread per padded slot, the vector maximum of field 14
+// over the aligned group of 8 slots (lanes 8k..8k+7 of a warp).
+__global__ void k_soa_records(const char * __restrict__ soa, const SoaOffsets o, int npad,
+                              double * __restrict__ rec)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = s < npad;
+    auto A = [&](long long off) { return __ldg((const double *)(soa + off) + s); };
+    const double sc = (in && o.screen >= 0) ? A(o.screen) : 0.0;
+    double m = sc;
+    #pragma unroll
+    for(int d = 1; d < 8; d <<= 1)
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, d));
+    if(!in)
+        return;
+    double * r = rec + (size_t)s * SB_REC;
+    r[0] = A(o.alpha); r[1] = A(o.prefac);
+    r[2] = A(o.x); r[3] = A(o.y); r[4] = A(o.z);
+    r[5] = A(o.pax); r[6] = A(o.pay); r[7] = A(o.paz);
+    r[8] = A(o.pbx); r[9] = A(o.pby); r[10] = A(o.pbz);
+    r[11] = o.a2 >= 0 ? A(o.a2) : 0.0;
+    r[12] = o.b2 >= 0 ? A(o.b2) : 0.0;
+    r[13] = sc;
+    r[14] = fmax(m, 0.0);
+    r[15] = o.screen >= 0 ? sqrt(fmax(sc, 0.0)) : INFINITY;
+}
+
+__global__ void k_soa_meta(const char * __restrict__ soa, const SoaOffsets o, int npair, int * __restrict__ nprim,
+                           double * __restrict__ ab)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if(p >= npair)
+        return;
+    nprim[p] = __ldg((const int *)(soa + o.nprim12) + p);
+    ab[3 * p + 0] = __ldg((const double *)(soa + o.abx) + p);
+    ab[3 * p + 1] = __ldg((const double *)(soa + o.aby) + p);
+    ab[3 * p + 2] = __ldg((const double *)(soa + o.abz) + p);
+}
+
+// Pair set P (arrays in page-locked host memory) into the packed layout L at
+// dpack on `stream`: one DMA of its allocation into dsoa, the pair starts
+// from hstart (page-locked, start.size() ints, kept until the stream has
+// run), the records and metadata built on the device.
+int upload_pinned_pairs(const simint_multi_shellpair * P, const PackedLayout & L, const std::vector<int> & start,
+                        char * dpack, DevBuf & dsoa, int * hstart, cudaStream_t stream)
+{
+    if(!dsoa.reserve(P->memsize))
+    {
+        set_error("out of device memory for pair data");
+        return SIMINT_B200_ERR_CUDA;
+    }
+    const char * base = (const char *)P->ptr;
+    auto off = [&](const void * a) { return a ? (long long)((const char *)a - base) : -1LL; };
+    SoaOffsets o;
+    o.x = off(P->x); o.y = off(P->y); o.z = off(P->z);
+    o.pax = off(P->PA_x); o.pay = off(P->PA_y); o.paz = off(P->PA_z);
+    o.pbx = off(P->PB_x); o.pby = off(P->PB_y); o.pbz = off(P->PB_z);
+    o.alpha = off(P->alpha); o.prefac = off(P->prefac); o.screen = off(P->screen);
+    o.a2 = off(P->alpha2); o.b2 = off(P->beta2);
+    o.abx = off(P->AB_x); o.aby = off(P->AB_y); o.abz = off(P->AB_z); o.nprim12 = off(P->nprim12);
+    cudaMemcpyAsync(dsoa.ptr, P->ptr, P->memsize, cudaMemcpyHostToDevice, stream);
+    memcpy(hstart, start.data(), (size_t)L.npair * sizeof(int));
+    cudaMemcpyAsync(dpack + L.off_start, hstart, (size_t)L.npair * sizeof(int), cudaMemcpyHostToDevice, stream);
+    k_soa_records<<<(unsigned)((L.npad + 255) / 256), 256, 0, stream>>>((const char *)dsoa.ptr, o, L.npad,
+                                                                      (double *)(dpack + L.off_rec));
+    k_soa_meta<<<(unsigned)((L.npair + 255) / 256), 256, 0, stream>>>((const char *)dsoa.ptr, o, L.npair,
+                                                                    (int *)(dpack + L.off_nprim),
+                                                                    (double *)(dpack + L.off_AB));
+    count_launch(2);
+    return 0;
+}
+
 PairSetDev device_view(const char * base, const PackedLayout & L, double screen_max)
 {
     PairSetDev d;
@@ -726,14 +805,34 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
     CallTrace tr;
     char * h = (char *)w.hstage.ptr;
     char * d = (char *)w.dpair.ptr;
+    const bool pinP = pair_data_pinned(P), pinQ = pair_data_pinned(Q);
+    std::vector<int> pstart;
+    if(pinP)
+        pack_layout(P, LP, &pstart);
     tr.time(tr.pack, [&] {
-        pack_pairs(P, h, LP);
-        pack_meta(Q, LQ, qstart, h + szP);
+        if(!pinP)
+            pack_pairs(P, h, LP);
+        if(!pinQ)
+            pack_meta(Q, LQ, qstart, h + szP);
     });
-    // P, and Q's starts/counts/AB (everything after the records)
-    cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream);
-    cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start, cudaMemcpyHostToDevice,
-                    w.stream);
+    if(pinP || pinQ)
+    {
+        if(!w.dsoa.reserve(std::max(pinP ? P->memsize : 0, pinQ ? Q->memsize : 0)))
+        {
+            set_error("out of device memory for pair data");
+            return SIMINT_B200_ERR_CUDA;
+        }
+    }
+    // P, and Q's starts/counts/AB (everything after the records); a pinned
+    // Q goes up whole, its records built on the device
+    int rc0 = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
+                   : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
+    if(rc0 == 0)
+        rc0 = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
+                   : (cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start,
+                                      cudaMemcpyHostToDevice, w.stream), 0);
+    if(rc0 != 0)
+        return rc0;
     const PairSetDev dP = device_view(d, LP, P->screen_max);
     const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
     int * dkord = (int *)(d + szP + szQ);
@@ -774,15 +873,17 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         char * hs = h + szP + szQ + (size_t)(k & 1) * slot;
         if(k >= 2)
             tr.time(tr.wait, [&] { cudaEventSynchronize(ev[k & 1]); });   // staging slot of chunk k-2 uploaded
-        const size_t recbytes = (size_t)(g1 - g0) * SB_REC * sizeof(double);
+        const size_t recbytes = pinQ ? 0 : (size_t)(g1 - g0) * SB_REC * sizeof(double);
         int * kk = (int *)(hs + recbytes);
         tr.time(tr.pack, [&] {
-            pack_records(Q, LQ.npad, g0, g1, (double *)hs);
+            if(!pinQ)
+                pack_records(Q, LQ.npad, g0, g1, (double *)hs);
             for(int q = c0; q < c1; q++) kk[q - c0] = q;
             std::stable_sort(kk, kk + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
         });
-        cudaMemcpyAsync(d + szP + (size_t)g0 * SB_REC * sizeof(double), hs, recbytes, cudaMemcpyHostToDevice,
-                        w.stream);
+        if(recbytes)
+            cudaMemcpyAsync(d + szP + (size_t)g0 * SB_REC * sizeof(double), hs, recbytes, cudaMemcpyHostToDevice,
+                            w.stream);
         cudaMemcpyAsync(dkord + c0, kk, (size_t)(c1 - c0) * sizeof(int), cudaMemcpyHostToDevice, w.stream);
         cudaEventRecord(ev[k & 1], w.stream);
         rc = launch_rectangle(P, dP, Q, dQ, dkord + c0, screen_tol, deriv, precision(), gate(),
@@ -864,8 +965,12 @@ extern "C" int simint_compute_eri_deriv(int deriv,
             return compute_eri_pipelined(deriv, P, Q, screen_tol, integrals, nc);
     }
     PackedLayout LP, LQ;
-    const size_t szP = (pack_pairs(P, nullptr, LP) + 255) & ~(size_t)255;
-    const size_t szQ = (pack_pairs(Q, nullptr, LQ) + 255) & ~(size_t)255;
+    std::vector<int> pstart, qstart;
+    const size_t szP = (pack_layout(P, LP, &pstart) + 255) & ~(size_t)255;
+    const size_t szQ = (pack_layout(Q, LQ, &qstart) + 255) & ~(size_t)255;
+    // pair sets in page-locked memory go up as their arrays in one DMA and
+    // become records on the device; the others are packed on the host
+    const bool pinP = pair_data_pinned(P), pinQ = pair_data_pinned(Q);
     // ket order: by primitive count (descending), stable
     std::vector<int> kord(Q->nshell12_clip);
     for(int k = 0; k < Q->nshell12_clip; k++) kord[k] = k;
@@ -879,12 +984,38 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     CallTrace tr;
     char * h = (char *)w.hstage.ptr;
     tr.time(tr.pack, [&] {
-        pack_pairs(P, h, LP);
-        pack_pairs(Q, h + szP, LQ);
+        if(!pinP)
+        {
+            pack_records(P, LP.npad, 0, LP.npad, (double *)(h + LP.off_rec));
+            pack_meta(P, LP, pstart, h);
+        }
+        if(!pinQ)
+        {
+            pack_records(Q, LQ.npad, 0, LQ.npad, (double *)(h + szP + LQ.off_rec));
+            pack_meta(Q, LQ, qstart, h + szP);
+        }
         memcpy(h + szP + szQ, kord.data(), kord.size() * sizeof(int));
     });
     char * d = (char *)w.dpair.ptr;
-    cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
+    if(pinP || pinQ)
+    {
+        if(!w.dsoa.reserve(std::max(pinP ? P->memsize : 0, pinQ ? Q->memsize : 0)))
+        {
+            set_error("out of device memory for pair data");
+            return SIMINT_B200_ERR_CUDA;
+        }
+        // the unused host staging of a pinned set holds its pair starts
+        int rc = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
+                      : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
+        if(rc == 0)
+            rc = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
+                      : (cudaMemcpyAsync(d + szP, h + szP, szQ, cudaMemcpyHostToDevice, w.stream), 0);
+        if(rc != 0)
+            return rc;
+        cudaMemcpyAsync(d + szP + szQ, h + szP + szQ, szK, cudaMemcpyHostToDevice, w.stream);
+    }
+    else
+        cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
     const PairSetDev dP = device_view(d, LP, P->screen_max);
     const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
     const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);

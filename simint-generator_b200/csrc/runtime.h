@@ -39,6 +39,7 @@ struct Workspace
     cudaStream_t stream = nullptr;
     cudaStream_t dstream = nullptr;       // downloads of pipelined calls
     DevBuf dpair, dout, dkord, dscratch;
+    DevBuf dsoa;                          // pair arrays copied from page-locked host memory
     HostBuf hstage, hout;
     ~Workspace();
 };
@@ -81,6 +82,9 @@ void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, do
 int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
                  cudaStream_t stream);
 bool class_uses_queue(const int req[4], int deriv, int prec);
+// Whether P's arrays live in page-locked host memory (large pair sets made
+// by simint_create_multi_shellpair; shell.cpp).
+bool pair_data_pinned(const simint_multi_shellpair * P);
 void permute_multi_shellpair(const simint_multi_shellpair * src, const int * order, simint_multi_shellpair * dst);
 void ssss_clip_vector(const simint_multi_shellpair * P, const simint_multi_shellpair * Q, int & v0, int & v1);
 

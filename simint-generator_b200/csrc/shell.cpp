@@ -13,10 +13,81 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <unordered_set>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "simint/simint.h"
 #include "simint_b200.h"
+
+// Pair data of at least this many bytes lives in page-locked host memory
+// (when a CUDA device is present and SIMINT_B200_PIN_PAIRS is not 0): the
+// compute calls then copy a pair set's arrays to the device with one DMA
+// and build the device records there, instead of packing them on the host.
+#define PAIR_PIN_MIN ((size_t)256 << 10)
+
+namespace {
+std::mutex g_pin_mutex;
+std::unordered_set<const void *> g_pinned;
+
+bool pin_enabled()
+{
+    static const bool on = [] {
+        const char * e = getenv("SIMINT_B200_PIN_PAIRS");
+        if(e && atoi(e) == 0)
+            return false;
+        int n = 0;
+        if(cudaGetDeviceCount(&n) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return false;
+        }
+        return n > 0;
+    }();
+    return on;
+}
+
+void * pair_alloc(size_t n)
+{
+    if(n >= PAIR_PIN_MIN && pin_enabled())
+    {
+        void * p = nullptr;
+        if(cudaHostAlloc(&p, n, cudaHostAllocPortable) == cudaSuccess)
+        {
+            std::lock_guard<std::mutex> lk(g_pin_mutex);
+            g_pinned.insert(p);
+            return p;
+        }
+        cudaGetLastError();
+    }
+    return SIMINT_ALLOC(n);
+}
+
+void pair_free(void * p)
+{
+    bool pinned;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mutex);
+        pinned = g_pinned.erase(p) > 0;
+    }
+    if(pinned)
+        cudaFreeHost(p);
+    else
+        SIMINT_FREE(p);
+}
+} // namespace
+
+namespace sb200 {
+bool pair_data_pinned(const simint_multi_shellpair * P)
+{
+    if(!P->ptr)
+        return false;
+    std::lock_guard<std::mutex> lk(g_pin_mutex);
+    return g_pinned.count(P->ptr) > 0;
+}
+}
 
 #define SQRT_TWO_PI_52 5.91496717279561287782347843505365022963403204272156069835237
 #define SQRT_TWO_TIMES_PI_52 24.739429451193148050228357586821944304008810699990039583
@@ -137,7 +208,7 @@ void simint_initialize_multi_shellpairs(int n, struct simint_multi_shellpair * P
 void simint_free_multi_shellpair(struct simint_multi_shellpair * P)
 {
     if(P->ptr != NULL)
-        SIMINT_FREE(P->ptr);
+        pair_free(P->ptr);
     simint_initialize_multi_shellpair(P);
 }
 
@@ -160,7 +231,7 @@ static void allocate_base(int npair, int nprim, struct simint_multi_shellpair * 
     if(P->memsize < memsize)
     {
         simint_free_multi_shellpair(P);
-        P->ptr = SIMINT_ALLOC(memsize);
+        P->ptr = pair_alloc(memsize);
         P->memsize = memsize;
     }
     char * base = (char *)P->ptr;

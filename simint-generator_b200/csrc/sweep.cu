@@ -654,6 +654,21 @@ extern "C" int simint_b200_basis_quartet(simint_b200_basis const * b, int k, lon
     return 0;
 }
 
+extern "C" int simint_b200_basis_class_kets(simint_b200_basis const * b, int k, int * shells)
+{
+    if(!b || k < 0 || k >= (int)b->qcs.size())
+        return SIMINT_B200_ERR_ARG;
+    const PairClass & Y = b->pcs[b->qcs[k].ky];
+    const int n = (int)Y.sa.size();
+    if(shells)
+        for(int i = 0; i < n; i++)
+        {
+            shells[2 * i] = Y.sa[(size_t)Y.order[(size_t)i]];
+            shells[2 * i + 1] = Y.sb[(size_t)Y.order[(size_t)i]];
+        }
+    return n;
+}
+
 extern "C" int simint_b200_basis_class_quartets(simint_b200_basis const * b, int k, int * sh)
 {
     if(!b || !sh || k < 0 || k >= (int)b->qcs.size())
@@ -698,7 +713,12 @@ static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout,
     double * dsums = (double *)b->dsums.ptr;
     QClass & q = b->qcs[k];
     const long long chunk = full ? q.ntask : std::max<long long>(1, cap / q.nout);
-    const bool queued = class_uses_queue(q.req, 0, prec);
+    // SIMINT_B200_SWEEP_QUEUE=0: static grid-stride task order instead
+    static const bool queue_on = [] {
+        const char * e = getenv("SIMINT_B200_SWEEP_QUEUE");
+        return !(e && atoi(e) == 0);
+    }();
+    const bool queued = queue_on && class_uses_queue(q.req, 0, prec);
     for(long long t0 = 0; t0 < q.ntask; t0 += chunk)
     {
         const long long cn = std::min(chunk, q.ntask - t0);

@@ -297,6 +297,16 @@ class Basis:
             raise IndexError(k)
         return sh[:nquart]
 
+    def class_kets(self, k):
+        """(n, 2) int array: the ket pair list of class k in stored order."""
+        self.lib.simint_b200_basis_class_kets.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        n = self.lib.simint_b200_basis_class_kets(self.h, k, None)
+        if n < 0:
+            raise IndexError(k)
+        sh = np.zeros((max(n, 1), 2), dtype=np.int32)
+        self.lib.simint_b200_basis_class_kets(self.h, k, C.c_void_p(sh.ctypes.data))
+        return sh[:n]
+
     def compute(self, prec, dev_ptr, ndoubles, stream=0):
         r = self.lib.simint_b200_basis_compute(self.h, prec, C.c_void_p(dev_ptr), ndoubles,
                                                C.c_void_p(stream))

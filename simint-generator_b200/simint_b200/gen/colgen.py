@@ -20,10 +20,13 @@ the right, Makowski.hpp:113-117):
 The first three terms read the thread's own registers; only the last reads
 another thread's column (the level below), through shared memory.  The
 columns' starting values (g_e, 0|0)^(m) come from the bra-only recursion,
-run beforehand level by level (colkern.cuh, col_f0).  The ket levels run as
-stages f = 1..c+d, one barrier each: stage f reads the orders 1.. of stage
-f-1 that other threads stored and stores its own for stage f+1.  The top
-quartets (e >= a, f >= c, m = 0) are summed in registers across batches.
+run beforehand for a block of up to 32 primitive quartets at once, level by
+level (colkern.cuh, col_f0_block); the block's values stay in shared memory
+(level-major: level e holds orders 0..L-e of its nc(e) functions) while its
+batches of NP primitive quartets run the ket stages f = 1..c+d, one barrier
+each: stage f reads the orders 1.. of stage f-1 that other threads stored
+and stores its own for stage f+1.  The top quartets (e >= a, f >= c,
+m = 0) are summed in registers across batches.
 
 This file emits, per class, a traits struct with the class constants, the
 shared-memory sizes and the straight-line stage code, plus the kernel
@@ -75,11 +78,16 @@ def col_supported(am):
 def sizes(am):
     a, b, c, d = am
     E, F = a + b, c + d
+    L = E + F
     nrole = lo_h(E + 1)
-    f0n = (E + F + 1) * nrole
+    # level-major bra block: level e holds orders 0..L-e of nc(e) functions
+    lb = [0]
+    for e in range(E + 1):
+        lb.append(lb[-1] + nc(e) * (L - e + 1))
     sa = max([nc(f) * (F - f) * nrole for f in range(1, F + 1, 2)] + [0])
     sb = max([nc(f) * (F - f) * nrole for f in range(2, F + 1, 2)] + [0])
-    return dict(E=E, F=F, L=E + F, NROLE=nrole, NTOP=lo_h(F + 1) - lo_h(c), F0N=f0n, SAN=sa, SBN=sb)
+    return dict(E=E, F=F, L=L, NROLE=nrole, NTOP=lo_h(F + 1) - lo_h(c), F0B=lb[-1], LB=lb[:-1],
+                SAN=sa, SBN=sb)
 
 
 def emit_stages(am):
@@ -93,21 +101,22 @@ def emit_stages(am):
     reg = lambda f, p, m: "r%d_%d_%d" % (f, p, m)
     w("    template<typename T, int NP>")
     w("    __device__ static __forceinline__ void stages(const T * __restrict__ F0, T * __restrict__ SA,")
-    w("        T * __restrict__ SB, int own, const int (&loff)[3], const T (&XQ)[3], const T (&YQ)[3],")
-    w("        T Zq, const T (&kq)[KQN], const T (&cB)[3], bool valid, double (&acc)[NTOP])")
+    w("        T * __restrict__ SB, int own, int ownF, int ostr, const int (&loff)[3], const int (&loffF)[3],")
+    w("        const int (&mstrF)[3], const T (&XQ)[3], const T (&YQ)[3], T Zq, const T (&kq)[KQN],")
+    w("        const T (&cB)[3], bool valid, double (&acc)[NTOP])")
     w("    {")
     w("        constexpr int RS = NROLE * NP;")
-    # own f = 0 column, orders 0..F
+    # own f = 0 column, orders 0..F (from the block)
     w("        T %s;" % ", ".join(reg(0, 0, m) for m in range(F + 1)))
     w("        if(valid)")
     w("        {")
     for m in range(F + 1):
-        w("            %s = F0[%d * RS + own];" % (reg(0, 0, m), m))
+        w("            %s = F0[ownF + %d * ostr];" % (reg(0, 0, m), m))
     if c == 0:
         w("            acc[0] += (double)%s;" % reg(0, 0, 0))
     w("        }")
     for f in range(1, F + 1):
-        area_in = "F0" if f == 1 else ("SA" if (f - 1) % 2 == 1 else "SB")
+        area_in = "SA" if (f - 1) % 2 == 1 else "SB"
         area_out = "SA" if f % 2 == 1 else "SB"
         nm = F - f + 1                          # orders of block f: 0..F-f
         names = []
@@ -130,13 +139,15 @@ def emit_stages(am):
                 if nA > 0:
                     e = "cfma(kq[%d], cfma(Zq, %s, %s), %s)" % (nA - 1, reg(f - 2, p2, m + 1),
                                                               reg(f - 2, p2, m), e)
-                # s3: (e - 1_y, f - 1_y)^(m+1) of the level below, stored by
-                # stage f - 1 (orders 1.. of block f - 1), or the f = 0 columns
+                # s3: (e - 1_y, f - 1_y)^(m+1) of the level below: from the
+                # bra block for f = 1, else stored by stage f - 1 (orders
+                # 1.. of block f - 1)
                 if f == 1:
-                    cst = (m + 1) * NR
+                    s3 = "F0[loffF[%d] + %d * mstrF[%d]]" % (y, m + 1, y)
                 else:
                     cst = (p1 * (F - f + 1) + m) * NR
-                e = "cfma(cB[%d], %s[%d * NP + loff[%d]], %s)" % (y, area_in, cst, y, e)
+                    s3 = "%s[%d * NP + loff[%d]]" % (area_in, cst, y)
+                e = "cfma(cB[%d], %s, %s)" % (y, s3, e)
                 body.append("            %s = %s;" % (r, e))
                 if m >= 1 and f <= F - 1:
                     body.append("            %s[%d * RS + own] = %s;" % (area_out, (p_ * (F - f) + m - 1), r))
@@ -167,7 +178,7 @@ def emit_traits(am):
     w("    static constexpr int E = %d, F = %d, L = %d;" % (z["E"], z["F"], z["L"]))
     w("    static constexpr int NROLE = %d, NTOP = %d, KQN = %d;" % (z["NROLE"], z["NTOP"],
                                                                    max(1, z["F"] - 1)))
-    w("    static constexpr int F0N = %d, SAN = %d, SBN = %d;" % (z["F0N"], z["SAN"], z["SBN"]))
+    w("    static constexpr int F0B = %d, SAN = %d, SBN = %d;" % (z["F0B"], z["SAN"], z["SBN"]))
     o.extend(emit_stages(am))
     w("};")
     return "\n".join(o)

