@@ -16,9 +16,9 @@ Outputs (numpy .npz, a few hundred kB in total):
   valeev_deriv0.npz  every class up to (dd|dd), Psi4 order
   valeev_deriv1.npz  every class up to (pp|pp) and a set of d classes
   valeev_fg.npz      f and g classes (deriv 0) with 1-3 primitives, exponents
-                     in [0.05, 5e4] (the benchmark configurations' range) and
-                     shells on two pseudo-atoms in a 2.5 bohr box; ValeevRef in
-                     Psi4 order
+                     in [0.05, 5e4] (the benchmark configurations' range; each
+                     shell's first primitive diffuse, 0.05-5) and shells on two
+                     pseudo-atoms in a 2 bohr box; ValeevRef in Psi4 order
   valeev_fg_d1.npz   f classes, deriv 1, the same ranges
   boys_ref.npz       reference boys_F_split values and grid rows
   pairs_ref.npz      reference multi-shell-pair arrays (no screening and
@@ -76,12 +76,15 @@ def valeev(ref, S, grp, deriv):
     return out
 
 
-def make_valeev(ref, deriv, classes, nsh, nprim, seed, alpha=(0.15, 12.0), box=2.5, natom=None):
+def make_valeev(ref, deriv, classes, nsh, nprim, seed, alpha=(0.15, 12.0), box=2.5, shell_fn=None):
     rng = np.random.default_rng(seed)
     data = {}
     for am in classes:
         ams = sum(([am[k]] * nsh[k] for k in range(4)), [])
-        shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box, natom=natom)
+        if shell_fn:
+            shells = shell_fn(rng, ams, nprim=nprim)
+        else:
+            shells = random_shells(rng, ams, nprim_range=nprim, alpha=alpha, box=box)
         S = normalized(ref, shells)
         # store the normalised coefficients so users skip normalisation
         norm = [(s[0], s[1], s[2], S.coefs(k)) for k, s in enumerate(shells)]
@@ -203,14 +206,28 @@ FG_D0 = [(3, 0, 0, 0), (3, 0, 3, 0), (3, 1, 3, 0), (3, 2, 1, 1), (3, 2, 2, 1), (
 FG_D1 = [(3, 0, 0, 0), (3, 1, 1, 0), (3, 2, 1, 1), (3, 1, 2, 2), (2, 2, 3, 0)]
 
 
+def fg_shells(rng, ams, nprim=(1, 3), alpha=(0.05, 5e4), box=2.0, natom=2):
+    """Shells for the f/g fixtures: exponents log-uniform over the
+    configurations' range, except that every shell's first primitive is
+    diffuse (0.05-5), as in contracted shells, so that quartets across the
+    two pseudo-atoms do not all underflow."""
+    atoms = rng.uniform(0.0, box, size=(natom, 3))
+    out = []
+    for k, am in enumerate(ams):
+        n = int(rng.integers(nprim[0], nprim[1] + 1))
+        al = np.exp(rng.uniform(np.log(alpha[0]), np.log(alpha[1]), size=n))
+        al[0] = np.exp(rng.uniform(np.log(0.05), np.log(5.0)))
+        co = rng.uniform(0.1, 1.0, size=n)
+        out.append((int(am), tuple(atoms[k % natom]), al, co))
+    return out
+
+
 def _fg_one(job):
     """One f/g class in a worker process (its own reference library handle
     and a seed of its own, so the result does not depend on the order)."""
     deriv, am, nsh, nprim, seed = job
     ref = load_ref()
-    # two pseudo-atoms: tight primitives (up to 5e4) on shared centres keep
-    # the integrals far from underflow
-    return make_valeev(ref, deriv, [am], nsh, nprim, seed, alpha=(0.05, 5e4), box=2.5, natom=2)
+    return make_valeev(ref, deriv, [am], nsh, nprim, seed, shell_fn=fg_shells)
 
 
 def make_fg(ref, workers=None):
