@@ -389,7 +389,8 @@ double rd_rows(int nrow, const int * bh, const int * kh, const int * kc, int der
             const int cend = (out && g_scr0[kh[r]] && tol > 0.0) ? ssss_clip_end(P, &Q) : -1;
             if(cend >= 0)
             {
-                const size_t n = (size_t)SIMINT_SIMD_ROUND(cend);
+                /* the whole array: a library may read every slot */
+                const size_t n = (size_t)padded_slots(&Q);
                 if(n > scr_cap)
                 {
                     free(scr);

@@ -210,7 +210,8 @@ def compare_class(ref_out, ref_keys, ref_offs, dev_vals, sh4, nout, nshell, chun
     with the reference's values of the same quartets.  Quartets the
     reference rows do not hold (a different cut at the screening boundary)
     are skipped.  Returns (max abs, max rel over |ref| > 1e-15, number
-    compared, number of bar failures: abs > 1e-13 and rel > 1e-11)."""
+    compared, number of elements beyond the bar: abs > 1e-13 and rel >
+    1e-11, number of quartets holding such an element)."""
     sh = sh4.astype(np.int64)
     keys = ((sh[:, 0] * nshell + sh[:, 1]) * nshell + sh[:, 2]) * nshell + sh[:, 3]
     pos = np.searchsorted(ref_keys, keys)
@@ -218,7 +219,7 @@ def compare_class(ref_out, ref_keys, ref_offs, dev_vals, sh4, nout, nshell, chun
     hit = (len(ref_keys) > 0) & (ref_keys[pos] == keys) if len(ref_keys) else np.zeros(len(keys), bool)
     qidx = np.nonzero(hit)[0]
     mabs = mrel = 0.0
-    nbad = 0
+    nbad = nbadq = 0
     cols = np.arange(nout, dtype=np.int64)
     for c0 in range(0, len(qidx), chunk):
         q = qidx[c0:c0 + chunk]
@@ -230,5 +231,7 @@ def compare_class(ref_out, ref_keys, ref_offs, dev_vals, sh4, nout, nshell, chun
         rel = np.where(big, d / np.where(big, ar, 1.0), 0.0)
         mabs = max(mabs, float(d.max()) if d.size else 0.0)
         mrel = max(mrel, float(rel.max()) if rel.size else 0.0)
-        nbad += int(np.count_nonzero((d > 1e-13) & ((~big) | (rel > 1e-11))))
-    return mabs, mrel, len(qidx), nbad
+        beyond = (d > 1e-13) & ((~big) | (rel > 1e-11))
+        nbad += int(np.count_nonzero(beyond))
+        nbadq += int(np.count_nonzero(beyond.any(axis=1)))
+    return mabs, mrel, len(qidx), nbad, nbadq

@@ -51,7 +51,7 @@ static bool col_layout(const ColKernels & k, const C2Params & p, int v, ColLayou
     const size_t acc = (size_t)((p.acc_size + 1) & ~1);
     for(int fs = 32; fs >= np; fs /= 2)
     {
-        int vd = std::max(k.f0b * fs + k.sab * np, k.red_per_np * np);
+        int vd = std::max(k.f0b * col_pitch(fs) + k.sab * np, k.red_per_np * np);
         vd = std::max(vd, p.hrr_need);
         vd = (vd + 1) & ~1;
         const size_t smem = ((size_t)vd + (size_t)k.ncoef * fs + acc) * sizeof(double) + 2 * (size_t)L.nt * sizeof(int);

@@ -91,16 +91,22 @@ __device__ __forceinline__ int col_stepdir(int i, int j, int k)
     return 0;
 }
 
-// Set-up and Boys values of survivors list[s0 .. s0 + FS) (FS threads in
-// parallel; slots past n get zeros, which run through the recursion as
+// Row pitch of the bra block for FS slots: FS + 8 doubles from 16 slots up,
+// so that the 8-slot segments of the four roles a warp reads fall on both
+// halves of the shared-memory banks (a multiple of 16 would put them all on
+// one half).
+__host__ __device__ constexpr int col_pitch(int FS) { return FS >= 16 ? FS + 8 : FS; }
+
+// Set-up and Boys values of survivors list[s0 .. s0 + ns) (ns <= FS threads
+// in parallel; slots past n get zeros, which run through the recursion as
 // zeros) into coef[k * FS + slot].
 template<class CT>
 __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
                                           int nj, unsigned long long njinv, bool fastdiv,
-                                          double * __restrict__ coef, int FS)
+                                          double * __restrict__ coef, int FS, int ns)
 {
     const int tid = threadIdx.x;
-    if(tid < FS)
+    if(tid < ns)
     {
         const int g = s0 + tid;
         double v[CC_F + CT::L + 1];
@@ -130,19 +136,20 @@ __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __re
     __syncthreads();
 }
 
-// Bra-only recursion of a block of FS primitive quartets into the
+// Bra-only recursion of the first ns slots of a block into the
 // level-major block F0: (g, 0|0)^(m) of bra function g = lo(e) + p at
-// F0[(lb(e) + m * nc(e) + p) * FS + slot], orders 0..L - e (level 0: F_m
+// F0[(lb(e) + m * nc(e) + p) * FR + slot], orders 0..L - e (level 0: F_m
 // times the pair prefactors).  Work items (function, slot) of a level spread
 // over the CTA; one barrier per level.
 template<typename T, class CT, int NT>
-__device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS)
+__device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS,
+                                             int FR, int ns)
 {
     const int tid = threadIdx.x;
-    for(int it = tid; it < (CT::L + 1) * FS; it += NT)
+    for(int it = tid; it < (CT::L + 1) * ns; it += NT)
     {
-        const int m = it / FS, slot = it - m * FS;
-        F0[m * FS + slot] = (T)coef[(CC_F + m) * FS + slot];
+        const int m = it / ns, slot = it - m * ns;
+        F0[m * FR + slot] = (T)coef[(CC_F + m) * FS + slot];
     }
     __syncthreads();
     int lb2 = 0, lb1 = 0, lbe = CT::L + 1;           // first rows of levels e-2, e-1, e
@@ -150,10 +157,10 @@ __device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double *
     for(int e = 1; e <= CT::E; e++)
     {
         const int nce = ((e + 1) * (e + 2)) / 2, nc1 = (e * (e + 1)) / 2, nc2 = ((e - 1) * e) / 2;
-        const int nitem = nce * FS;
+        const int nitem = nce * ns;
         for(int it = tid; it < nitem; it += NT)
         {
-            const int pe = it / FS, slot = it - pe * FS;
+            const int pe = it / ns, slot = it - pe * ns;
             int i, j, k, l;
             col_cart(col_lo(e) + pe, i, j, k, l);
             const int x = col_stepdir(i, j, k);
@@ -167,10 +174,10 @@ __device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double *
             const T YP = (T)coef[(CC_YP + x) * FS + slot];
             const T Zp = (T)coef[CC_ZP * FS + slot];
             const T k2 = (T)((double)n * coef[CC_O2P * FS + slot]);
-            const T * s1 = F0 + (lb1 + p1) * FS + slot;
-            const T * s2 = F0 + (n > 0 ? (lb2 + p2) * FS + slot : 0);
-            T * dst = F0 + (lbe + pe) * FS + slot;
-            const int st1 = nc1 * FS, st2 = nc2 * FS, st = nce * FS;
+            const T * s1 = F0 + (lb1 + p1) * FR + slot;
+            const T * s2 = F0 + (n > 0 ? (lb2 + p2) * FR + slot : 0);
+            T * dst = F0 + (lbe + pe) * FR + slot;
+            const int st1 = nc1 * FR, st2 = nc2 * FR, st = nce * FR;
             for(int m = 0; m <= CT::L - e; m++)
             {
                 T r = XP * s1[m * st1];
@@ -199,7 +206,7 @@ struct ColThread
 };
 
 template<class CT, int NP>
-__device__ __forceinline__ void col_thread(ColThread & t, int FS)
+__device__ __forceinline__ void col_thread(ColThread & t, int FR)
 {
     const int tid = threadIdx.x;
     t.role = tid / NP;
@@ -212,8 +219,8 @@ __device__ __forceinline__ void col_thread(ColThread & t, int FS)
     t.own = t.role * NP + t.slot;
     const int pe = t.valid ? t.role - col_lo(re) : 0;
     const int lbr = col_lb(CT::L, re), lbr1 = re > 0 ? col_lb(CT::L, re - 1) : 0;
-    t.ownF = t.valid ? (lbr + pe) * FS + t.slot : t.slot;
-    t.ostr = ((re + 1) * (re + 2)) / 2 * FS;
+    t.ownF = t.valid ? (lbr + pe) * FR + t.slot : t.slot;
+    t.ostr = ((re + 1) * (re + 2)) / 2 * FR;
     #pragma unroll
     for(int y = 0; y < 3; y++)
     {
@@ -224,8 +231,8 @@ __device__ __forceinline__ void col_thread(ColThread & t, int FS)
         // absent g_e - 1_y: the thread's own position (its coefficient n_y
         // is 0 and the value read is a finite one)
         t.loff[y] = (has ? g1 : (t.valid ? t.role : 0)) * NP + t.slot;
-        t.loffF[y] = has ? (lbr1 + g1 - col_lo(re - 1)) * FS + t.slot : t.ownF;
-        t.mstrF[y] = has ? (re * (re + 1)) / 2 * FS : t.ostr;
+        t.loffF[y] = has ? (lbr1 + g1 - col_lo(re - 1)) * FR + t.slot : t.ownF;
+        t.mstrF[y] = has ? (re * (re + 1)) / 2 * FR : t.ostr;
     }
 }
 
@@ -261,12 +268,16 @@ __device__ __forceinline__ void col_block(const QuartetCtx & c, const int * __re
                                           double * __restrict__ V, int FS, const ColThread & t,
                                           double (&acc)[CT::NTOP])
 {
+    const int FR = col_pitch(FS);
     T * F0 = (T *)V;
-    T * SA = F0 + CT::F0B * FS;
+    T * SA = F0 + CT::F0B * FR;
     T * SB = SA + CT::SAN * NP;
-    col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS);
-    col_f0_block<T, CT, NT>(F0, coef, FS);
+    // a short last block (or a short contraction) sets up and runs the
+    // bra recursion for its batches only
     const int nb = min(FS, n - s0);
+    const int ns = ((nb + NP - 1) / NP) * NP;
+    col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS, ns);
+    col_f0_block<T, CT, NT>(F0, coef, FS, FR, ns);
     for(int b0 = 0; b0 < nb; b0 += NP)
         col_batch<T, CT, NP>(F0, SA, SB, coef, FS, b0, t, acc);
 }
@@ -286,7 +297,7 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
     int * surv = (int *)(acc2 + ((p.acc_size + 1) & ~1));   // [0, NT): FP64 list, [NT, 2 NT): FP32 list
     const int tid = threadIdx.x;
     ColThread th;
-    col_thread<CT, NP>(th, FS);
+    col_thread<CT, NP>(th, col_pitch(FS));
     const int role = th.role, slot = th.slot;
     const bool valid = th.valid;
     const int lane = tid & 31, warp = tid >> 5;

@@ -427,6 +427,26 @@ __global__ void k_soa_meta(const char * __restrict__ soa, const SoaOffsets o, in
     ab[3 * p + 2] = __ldg((const double *)(soa + o.abz) + p);
 }
 
+// Whether every array of P lies inside its own allocation [ptr, ptr +
+// memsize) with its full extent (npad slots, npair pairs): only then is one
+// DMA of the allocation a copy of the pair set.  (A caller may point an
+// array elsewhere, e.g. at a private copy of the screening values.)
+bool pair_arrays_in_block(const simint_multi_shellpair * P, int npad)
+{
+    const char * b = (const char *)P->ptr;
+    const char * e = b + P->memsize;
+    auto in = [&](const void * a, size_t n) {
+        const char * c = (const char *)a;
+        return !a || (c >= b && c + n <= e);
+    };
+    const size_t dp = (size_t)npad * sizeof(double), dq = (size_t)P->nshell12 * sizeof(double);
+    return in(P->x, dp) && in(P->y, dp) && in(P->z, dp) && in(P->PA_x, dp) && in(P->PA_y, dp) &&
+           in(P->PA_z, dp) && in(P->PB_x, dp) && in(P->PB_y, dp) && in(P->PB_z, dp) && in(P->alpha, dp) &&
+           in(P->prefac, dp) && in(P->screen, dp) && in(P->alpha2, dp) && in(P->beta2, dp) &&
+           in(P->AB_x, dq) && in(P->AB_y, dq) && in(P->AB_z, dq) &&
+           in(P->nprim12, (size_t)P->nshell12 * sizeof(int)) && P->x && P->alpha && P->prefac && P->nprim12;
+}
+
 // Pair set P (arrays in page-locked host memory) into the packed layout L at
 // dpack on `stream`: one DMA of its allocation into dsoa, the pair starts
 // from hstart (page-locked, start.size() ints, kept until the stream has
@@ -805,7 +825,8 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
     CallTrace tr;
     char * h = (char *)w.hstage.ptr;
     char * d = (char *)w.dpair.ptr;
-    const bool pinP = pair_data_pinned(P), pinQ = pair_data_pinned(Q);
+    const bool pinP = pair_data_pinned(P) && pair_arrays_in_block(P, LP.npad);
+    const bool pinQ = pair_data_pinned(Q) && pair_arrays_in_block(Q, LQ.npad);
     std::vector<int> pstart;
     if(pinP)
         pack_layout(P, LP, &pstart);
@@ -970,7 +991,8 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     const size_t szQ = (pack_layout(Q, LQ, &qstart) + 255) & ~(size_t)255;
     // pair sets in page-locked memory go up as their arrays in one DMA and
     // become records on the device; the others are packed on the host
-    const bool pinP = pair_data_pinned(P), pinQ = pair_data_pinned(Q);
+    const bool pinP = pair_data_pinned(P) && pair_arrays_in_block(P, LP.npad);
+    const bool pinQ = pair_data_pinned(Q) && pair_arrays_in_block(Q, LQ.npad);
     // ket order: by primitive count (descending), stable
     std::vector<int> kord(Q->nshell12_clip);
     for(int k = 0; k < Q->nshell12_clip; k++) kord[k] = k;
