@@ -52,6 +52,14 @@ int simint_b200_get_ordering(void);
 int simint_b200_set_precision(int mode, double gate);
 int simint_b200_get_precision(void);
 
+/* Pair data placement: simint_create_multi_shellpair(2) and
+ * simint_cat_multi_shellpair allocate pair sets of 256 KB or more in
+ * page-locked host memory when a CUDA device is present (environment
+ * variable SIMINT_B200_PIN_PAIRS=0: never); simint_free_multi_shellpair
+ * frees them.  simint_compute_eri(_deriv) copies such a set to the device
+ * with one DMA of its allocation and builds the device records there;
+ * arrays a caller pointed outside the allocation are packed on the host. */
+
 /* Text of the last error seen by the calling thread. */
 const char * simint_b200_last_error(void);
 
