@@ -136,6 +136,64 @@ __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __re
     __syncthreads();
 }
 
+// Bra-only recursion of the first ns slots of a block into the
+// level-major block F0: (g, 0|0)^(m) of bra function g = lo(e) + p at
+// F0[(lb(e) + m * nc(e) + p) * FR + slot], orders 0..L - e (level 0: F_m
+// times the pair prefactors).  Work items (function, slot) of a level spread
+// over the CTA; one barrier per level.
+template<typename T, class CT, int NT>
+__device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS,
+                                             int FR, int ns)
+{
+    const int tid = threadIdx.x;
+    for(int it = tid; it < (CT::L + 1) * ns; it += NT)
+    {
+        const int m = it / ns, slot = it - m * ns;
+        F0[m * FR + slot] = (T)coef[(CC_F + m) * FS + slot];
+    }
+    __syncthreads();
+    int lb2 = 0, lb1 = 0, lbe = CT::L + 1;           // first rows of levels e-2, e-1, e
+    #pragma unroll 1
+    for(int e = 1; e <= CT::E; e++)
+    {
+        const int nce = ((e + 1) * (e + 2)) / 2, nc1 = (e * (e + 1)) / 2, nc2 = ((e - 1) * e) / 2;
+        const int nitem = nce * ns;
+        for(int it = tid; it < nitem; it += NT)
+        {
+            const int pe = it / ns, slot = it - pe * ns;
+            int i, j, k, l;
+            col_cart(col_lo(e) + pe, i, j, k, l);
+            const int x = col_stepdir(i, j, k);
+            int q[3] = {i, j, k};
+            const int n = q[x] - 1;
+            q[x] -= 1;
+            const int p1 = col_flat(q[0], q[1], q[2]) - col_lo(e - 1);
+            q[x] -= 1;
+            const int p2 = n > 0 ? col_flat(q[0], q[1], q[2]) - col_lo(e - 2) : 0;
+            const T XP = (T)coef[(CC_XP + x) * FS + slot];
+            const T YP = (T)coef[(CC_YP + x) * FS + slot];
+            const T Zp = (T)coef[CC_ZP * FS + slot];
+            const T k2 = (T)((double)n * coef[CC_O2P * FS + slot]);
+            const T * s1 = F0 + (lb1 + p1) * FR + slot;
+            const T * s2 = F0 + (n > 0 ? (lb2 + p2) * FR + slot : 0);
+            T * dst = F0 + (lbe + pe) * FR + slot;
+            const int st1 = nc1 * FR, st2 = nc2 * FR, st = nce * FR;
+            for(int m = 0; m <= CT::L - e; m++)
+            {
+                T r = XP * s1[m * st1];
+                r = cfma(YP, s1[(m + 1) * st1], r);
+                if(n > 0)
+                    r = cfma(k2, cfma(Zp, s2[(m + 1) * st2], s2[m * st2]), r);
+                dst[m * st] = r;
+            }
+        }
+        __syncthreads();
+        lb2 = lb1;
+        lb1 = lbe;
+        lbe += nce * (CT::L - e + 1);
+    }
+}
+
 // Per-thread constants of the column kernel: the thread's role (bra
 // function g_e) and slot, its positions in the batch areas (own, loff) and
 // in the bra block (ownF + m * ostr: order m of its own column; loffF[y] +
@@ -145,7 +203,6 @@ struct ColThread
     int role, slot, own, ownF, ostr;
     bool valid;
     int ny[3], loff[3], loffF[3], mstrF[3];
-    int re;                              // level of the thread's function (-1: no function)
 };
 
 template<class CT, int NP>
@@ -160,10 +217,8 @@ __device__ __forceinline__ void col_thread(ColThread & t, int FR)
         col_cart(t.role, ri, rj, rk, re);
     t.ny[0] = ri; t.ny[1] = rj; t.ny[2] = rk;
     t.own = t.role * NP + t.slot;
-    t.re = t.valid ? re : -1;
     const int pe = t.valid ? t.role - col_lo(re) : 0;
     const int lbr = col_lb(CT::L, re), lbr1 = re > 0 ? col_lb(CT::L, re - 1) : 0;
-
     t.ownF = t.valid ? (lbr + pe) * FR + t.slot : t.slot;
     t.ostr = ((re + 1) * (re + 2)) / 2 * FR;
     #pragma unroll
@@ -178,74 +233,6 @@ __device__ __forceinline__ void col_thread(ColThread & t, int FR)
         t.loff[y] = (has ? g1 : (t.valid ? t.role : 0)) * NP + t.slot;
         t.loffF[y] = has ? (lbr1 + g1 - col_lo(re - 1)) * FR + t.slot : t.ownF;
         t.mstrF[y] = has ? (re * (re + 1)) / 2 * FR : t.ostr;
-    }
-}
-
-// Bra-only recursion of the first ns slots of a block into the
-// level-major block F0: (g, 0|0)^(m) of bra function g = lo(e) + p at
-// F0[(lb(e) + m * nc(e) + p) * FR + slot], orders 0..L - e (level 0: F_m
-// times the pair prefactors).  Level by level, one barrier each; at level e
-// the NP threads of each function of that level compute it for slots
-// slot, slot + NP, ... (their step direction and source rows precomputed in
-// ColThread).
-template<typename T, class CT, int NP>
-__device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS,
-                                             int FR, int ns, const ColThread & t)
-{
-    if(t.re == 0)
-        for(int s = t.slot; s < ns; s += NP)
-        {
-            #pragma unroll
-            for(int m = 0; m <= CT::L; m++)
-                F0[m * FR + s] = (T)coef[(CC_F + m) * FS + s];
-        }
-    __syncthreads();
-    // the thread's own function: step direction x, n = (exponent - 1)
-    // along it, rows of g - 1_x and g - 2_x (levels e-1, e-2) in the block
-    int x = 0, n = 0, r1 = 0, r2 = 0, st1 = FR, st2 = FR;
-    if(t.re > 0)
-    {
-        int i, j, k, l;
-        col_cart(t.role, i, j, k, l);
-        x = col_stepdir(i, j, k);
-        int q[3] = {i, j, k};
-        n = q[x] - 1;
-        q[x] -= 1;
-        r1 = col_lb(CT::L, l - 1) + col_flat(q[0], q[1], q[2]) - col_lo(l - 1);
-        st1 = (l * (l + 1)) / 2 * FR;
-        if(n > 0)
-        {
-            q[x] -= 1;
-            r2 = col_lb(CT::L, l - 2) + col_flat(q[0], q[1], q[2]) - col_lo(l - 2);
-            st2 = ((l - 1) * l) / 2 * FR;
-        }
-    }
-    #pragma unroll 1
-    for(int e = 1; e <= CT::E; e++)
-    {
-        if(t.re == e)
-        {
-            const int st = t.ostr;
-            for(int s = t.slot; s < ns; s += NP)
-            {
-                const T XP = (T)coef[(CC_XP + x) * FS + s];
-                const T YP = (T)coef[(CC_YP + x) * FS + s];
-                const T Zp = (T)coef[CC_ZP * FS + s];
-                const T k2 = (T)((double)n * coef[CC_O2P * FS + s]);
-                const T * s1 = F0 + r1 * FR + s;
-                const T * s2 = F0 + r2 * FR + s;
-                T * dst = F0 + (t.ownF - t.slot) + s;
-                for(int m = 0; m <= CT::L - e; m++)
-                {
-                    T r = XP * s1[m * st1];
-                    r = cfma(YP, s1[(m + 1) * st1], r);
-                    if(n > 0)
-                        r = cfma(k2, cfma(Zp, s2[(m + 1) * st2], s2[m * st2]), r);
-                    dst[m * st] = r;
-                }
-            }
-        }
-        __syncthreads();
     }
 }
 
@@ -290,7 +277,7 @@ __device__ __forceinline__ void col_block(const QuartetCtx & c, const int * __re
     const int nb = min(FS, n - s0);
     const int ns = ((nb + NP - 1) / NP) * NP;
     col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS, ns);
-    col_f0_block<T, CT, NP>(F0, coef, FS, FR, ns, t);
+    col_f0_block<T, CT, NT>(F0, coef, FS, FR, ns);
     for(int b0 = 0; b0 < nb; b0 += NP)
         col_batch<T, CT, NP>(F0, SA, SB, coef, FS, b0, t, acc);
 }

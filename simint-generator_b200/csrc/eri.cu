@@ -614,6 +614,16 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         // untuned default: the register kernel while its contracted tops fit
         // registers (above ~200 accumulators it spills), else cooperative
         v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
+    // a small rectangle (one simint_compute_eri call) gives a thread-per-
+    // quartet kernel a handful of CTAs: the warp-per-quartet form of the
+    // same register kernel spreads it over 32x the threads
+    if(mode == 0 && a.ntask < 16384 && k && k->fnw[0][0])
+    {
+        if(v == VAR_STRAIGHT)
+            v = VAR_WARP;
+        else if(v == VAR_STRAIGHT64)
+            v = VAR_WARP64;
+    }
     if((v == VAR_STRAIGHT || v == VAR_STRAIGHT64) && k)
     {
         a.oidx = oidx_table(req, u, ordering());
@@ -1051,9 +1061,10 @@ extern "C" int simint_compute_eri_deriv(int deriv,
                              precision(), gate(), (double *)w.dout.ptr, w.stream);
     if(r < 0)
         return r;
-    // results through the pinned staging buffer (full-speed DMA), then into
-    // the caller's memory on all host cores
-    const bool staged = outbytes >= (1u << 20) && w.hout.reserve(outbytes);
+    // results through the pinned staging buffer (full-speed DMA; a copy
+    // into pageable memory would go through the driver's own staging), then
+    // into the caller's memory on all host cores
+    const bool staged = outbytes >= (64u << 10) && w.hout.reserve(outbytes);
     cudaMemcpyAsync(staged ? w.hout.ptr : (void *)integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost,
                     w.stream);
     cudaError_t e = cudaSuccess;
