@@ -176,7 +176,7 @@ int simint_b200_basis_queue_probe(simint_b200_basis * b, int k, long long publis
  * register kernel where one exists, thread- and warp-per-quartet; the
  * cooperative kernel with 256, 128 or 64 threads and 1, 2, 4 or 8
  * primitive quartets per wavefront pass; the column kernel with 4 or 8
- * primitive quartets per batch; in mixed mode each also in FP64) on the
+ * primitive quartets per batch, or 4 in two thread groups per CTA; in mixed mode each also in FP64) on the
  * sweep's own tasks and keep the fastest for `prec`.  Choices are process-wide and are written to the
  * JSON file $SIMINT_B200_TUNE_FILE when set (read back by simint_init). */
 int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
@@ -185,7 +185,9 @@ int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out
 /* The kernel variant chosen for a requested class (0 = untuned default,
  * 1 = register kernel, 20+B / 40+B / 60+B = cooperative kernel with 256 /
  * 128 / 64 threads and batch B = 1, 2, 4, 8, 81 / 82 = column kernel with
- * 4 / 8 primitive quartets per batch, deriv 0). */
+ * 4 / 8 primitive quartets per batch, 83 = column kernel with 4 per batch
+ * and two thread groups per CTA each running its own shell quartets,
+ * deriv 0). */
 int simint_b200_variant(const int am[4], int deriv, int prec);
 
 /* Pin the kernel variant of a requested class (same codes, plus 3 = first

@@ -32,33 +32,37 @@ bool col_is_variant(int v) { return v >= 81 && v <= 80 + COL_NNP; }
 
 struct ColLayout
 {
-    int npi, nt, vdoubles, fs;
+    int npi, nt, vdoubles, fs, phd;       // nt: threads per CTA; phd: shared doubles per group
     size_t smem;
 };
 
-// Shared memory of a launch: the recursion area V (the bra block of FS
-// primitive quartets and the stage areas of a batch of NP; also the
-// slot-sum and HRR scratch), the coefficient records of a block, the
-// accumulators of the HRR and the two survivor lists.  FS is the largest of
-// 32, 16, 8, 4 (a multiple of NP) that fits.
+// Shared memory of a launch, per group of threads: the recursion area V
+// (the bra block of FS primitive quartets and the stage areas of a batch of
+// NP; also the slot-sum and HRR scratch), the coefficient records of a
+// block, the accumulators of the HRR and the two survivor lists.  FS is the
+// largest of 32, 16, 8, 4 (a multiple of NP) for which the H groups fit.
 static bool col_layout(const ColKernels & k, const C2Params & p, int v, ColLayout & L)
 {
     L.npi = v - 81;
     if(L.npi < 0 || L.npi >= COL_NNP || !k.fn[L.npi][0][0])
         return false;
-    const int np = COL_NPS[L.npi];
-    L.nt = k.nt[L.npi];
-    const size_t acc = (size_t)((p.acc_size + 1) & ~1);
+    const int np = COL_NPS[L.npi], h = COL_HS[L.npi];
+    const int nth = k.nt[L.npi];
+    L.nt = h * nth;
+    const int acc = (p.acc_size + 1) & ~1;
     for(int fs = 32; fs >= np; fs /= 2)
     {
         int vd = std::max(k.f0b * col_pitch(fs) + k.sab * np, k.red_per_np * np);
         vd = std::max(vd, p.hrr_need);
         vd = (vd + 1) & ~1;
-        const size_t smem = ((size_t)vd + (size_t)k.ncoef * fs + acc) * sizeof(double) + 2 * (size_t)L.nt * sizeof(int);
+        // survivors: 2 nth ints = nth doubles
+        const int phd = (vd + k.ncoef * fs + acc + nth + 1) & ~1;
+        const size_t smem = (size_t)h * phd * sizeof(double);
         if(smem <= 220 * 1024)
         {
             L.fs = fs;
             L.vdoubles = vd;
+            L.phd = phd;
             L.smem = smem;
             return true;
         }
@@ -121,9 +125,11 @@ int launch_col(KernArgs & a, const int req[4], int mode, int prec, cudaStream_t 
         per_sm = it->second;
     }
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    long long grid = std::min<long long>(a.ntask, (long long)nsm * per_sm);
+    // each CTA runs H shell quartets at a time
+    const int h = COL_HS[L.npi];
+    long long grid = std::min<long long>((a.ntask + h - 1) / h, (long long)nsm * per_sm);
     grid = std::max<long long>(grid, 1);
-    fn<<<(unsigned)grid, L.nt, L.smem, stream>>>(a, p, L.vdoubles, L.fs);
+    fn<<<(unsigned)grid, L.nt, L.smem, stream>>>(a, p, L.vdoubles, L.fs, L.phd);
     count_launch(1);
     return 0;
 }

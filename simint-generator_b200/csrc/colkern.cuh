@@ -97,15 +97,30 @@ __device__ __forceinline__ int col_stepdir(int i, int j, int k)
 // one half).
 __host__ __device__ constexpr int col_pitch(int FS) { return FS >= 16 ? FS + 8 : FS; }
 
+// Barrier of one group of NTH threads of a CTA: group g waits on named
+// barrier 1 + g, so the H groups of a CTA run their shell quartets
+// independently (a CTA barrier when the CTA is one group).
+template<int H, int NTH>
+struct ColSync
+{
+    int id;
+    __device__ __forceinline__ void operator()() const
+    {
+        if constexpr(H == 1)
+            __syncthreads();
+        else
+            asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(NTH) : "memory");
+    }
+};
+
 // Set-up and Boys values of survivors list[s0 .. s0 + ns) (ns <= FS threads
 // in parallel; slots past n get zeros, which run through the recursion as
 // zeros) into coef[k * FS + slot].
-template<class CT>
+template<class CT, typename SYNC>
 __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
                                           int nj, unsigned long long njinv, bool fastdiv,
-                                          double * __restrict__ coef, int FS, int ns)
+                                          double * __restrict__ coef, int FS, int ns, int tid, SYNC sync)
 {
-    const int tid = threadIdx.x;
     if(tid < ns)
     {
         const int g = s0 + tid;
@@ -133,7 +148,7 @@ __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __re
         for(int k = 0; k < CC_F + CT::L + 1; k++)
             coef[k * FS + tid] = v[k];
     }
-    __syncthreads();
+    sync();
 }
 
 // Bra-only recursion of the first ns slots of a block into the
@@ -141,17 +156,16 @@ __device__ __forceinline__ void col_setup(const QuartetCtx & c, const int * __re
 // F0[(lb(e) + m * nc(e) + p) * FR + slot], orders 0..L - e (level 0: F_m
 // times the pair prefactors).  Work items (function, slot) of a level spread
 // over the CTA; one barrier per level.
-template<typename T, class CT, int NT>
+template<typename T, class CT, int NT, typename SYNC>
 __device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double * __restrict__ coef, int FS,
-                                             int FR, int ns)
+                                             int FR, int ns, int tid, SYNC sync)
 {
-    const int tid = threadIdx.x;
     for(int it = tid; it < (CT::L + 1) * ns; it += NT)
     {
         const int m = it / ns, slot = it - m * ns;
         F0[m * FR + slot] = (T)coef[(CC_F + m) * FS + slot];
     }
-    __syncthreads();
+    sync();
     int lb2 = 0, lb1 = 0, lbe = CT::L + 1;           // first rows of levels e-2, e-1, e
     #pragma unroll 1
     for(int e = 1; e <= CT::E; e++)
@@ -187,7 +201,7 @@ __device__ __forceinline__ void col_f0_block(T * __restrict__ F0, const double *
                 dst[m * st] = r;
             }
         }
-        __syncthreads();
+        sync();
         lb2 = lb1;
         lb1 = lbe;
         lbe += nce * (CT::L - e + 1);
@@ -206,9 +220,8 @@ struct ColThread
 };
 
 template<class CT, int NP>
-__device__ __forceinline__ void col_thread(ColThread & t, int FR)
+__device__ __forceinline__ void col_thread(ColThread & t, int FR, int tid)
 {
-    const int tid = threadIdx.x;
     t.role = tid / NP;
     t.slot = tid - t.role * NP;
     t.valid = t.role < CT::NROLE;
@@ -238,10 +251,10 @@ __device__ __forceinline__ void col_thread(ColThread & t, int FR)
 
 // The ket stages of batch [b0, b0 + NP) of a block (coef: the block's
 // records, row stride FS) in type T.
-template<typename T, class CT, int NP>
+template<typename T, class CT, int NP, typename SYNC>
 __device__ __forceinline__ void col_batch(const T * __restrict__ F0, T * __restrict__ SA, T * __restrict__ SB,
                                           const double * __restrict__ coef, int FS, int b0,
-                                          const ColThread & t, double (&acc)[CT::NTOP])
+                                          const ColThread & t, double (&acc)[CT::NTOP], SYNC sync)
 {
     const int cs = b0 + t.slot;
     T XQ[3], YQ[3], cB[3], kq[CT::KQN], Zq = 0;
@@ -258,15 +271,15 @@ __device__ __forceinline__ void col_batch(const T * __restrict__ F0, T * __restr
     for(int k = 0; k < CT::KQN; k++)
         kq[k] = t.valid ? (T)((double)(k + 1) * coef[CC_O2Q * FS + cs]) : (T)0;
     CT::template stages<T, NP>(F0 + b0, SA, SB, t.own, t.ownF, t.ostr, t.loff, t.loffF, t.mstrF, XQ, YQ, Zq, kq,
-                               cB, t.valid, acc);
+                               cB, t.valid, acc, sync);
 }
 
 // One block of survivors list[s0 ..) in type T: set-up, bra block, batches.
-template<typename T, class CT, int NP, int NT>
+template<typename T, class CT, int NP, int NT, typename SYNC>
 __device__ __forceinline__ void col_block(const QuartetCtx & c, const int * __restrict__ list, int s0, int n,
                                           int nj, unsigned long long njinv, bool fastdiv, double * __restrict__ coef,
                                           double * __restrict__ V, int FS, const ColThread & t,
-                                          double (&acc)[CT::NTOP])
+                                          double (&acc)[CT::NTOP], int tid, SYNC sync)
 {
     const int FR = col_pitch(FS);
     T * F0 = (T *)V;
@@ -276,33 +289,63 @@ __device__ __forceinline__ void col_block(const QuartetCtx & c, const int * __re
     // bra recursion for its batches only
     const int nb = min(FS, n - s0);
     const int ns = ((nb + NP - 1) / NP) * NP;
-    col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS, ns);
-    col_f0_block<T, CT, NT>(F0, coef, FS, FR, ns);
+    col_setup<CT>(c, list, s0, n, nj, njinv, fastdiv, coef, FS, ns, tid, sync);
+    col_f0_block<T, CT, NT>(F0, coef, FS, FR, ns, tid, sync);
     for(int b0 = 0; b0 < nb; b0 += NP)
-        col_batch<T, CT, NP>(F0, SA, SB, coef, FS, b0, t, acc);
+        col_batch<T, CT, NP>(F0, SA, SB, coef, FS, b0, t, acc, sync);
 }
 
-template<class CT, int MODE, bool MIXED, int NP>
-__global__ void __launch_bounds__(col_nt(CT::NROLE, NP), 1)
-k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
+// Task loop of one group: static stride over the group slots of the grid,
+// or pulls from the launch's work queue (thread 0 of the group pulls).
+template<typename SYNC>
+__device__ __forceinline__ bool col_next_task(const KernArgs & a, long long & slot, long long & t,
+                                              long long * s_slot, int tid, SYNC sync)
 {
-    constexpr int NT = col_nt(CT::NROLE, NP);
+    if(a.wq)
+    {
+        if(tid == 0)
+            *s_slot = queue_pull(a.wq);
+        sync();
+        slot = *s_slot;
+        sync();
+        if(slot < 0)
+            return false;
+    }
+    else if(slot >= a.ntask)
+        return false;
+    t = a.tperm ? (long long)__ldg(a.tperm + slot) : slot;
+    return true;
+}
+
+// H groups of NT threads per CTA (H = 1 or 2), each with its own part of
+// shared memory (phd doubles) running its own shell quartets: while one
+// group waits at a barrier the other computes.
+template<class CT, int MODE, bool MIXED, int NP, int H>
+__global__ void __launch_bounds__(H * col_nt(CT::NROLE, NP), 1)
+k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS, const int phd)
+{
+    constexpr int NT = col_nt(CT::NROLE, NP);       // threads of a group
     extern __shared__ __align__(16) double sm[];
-    __shared__ int wcount[2][NT / 32];
-    __shared__ int s_cnt[2];
-    __shared__ long long s_qslot;
-    double * V = sm;
-    double * coef = sm + vdoubles;
+    __shared__ int wcount_g[H][2][NT / 32];
+    __shared__ int s_cnt_g[H][2];
+    __shared__ long long s_qslot_g[H];
+    const int grp = H == 1 ? 0 : (int)threadIdx.x / NT;
+    const int tid = (int)threadIdx.x - grp * NT;
+    const ColSync<H, NT> sync{1 + grp};
+    int (*wcount)[NT / 32] = wcount_g[grp];
+    int * s_cnt = s_cnt_g[grp];
+    double * V = sm + (size_t)grp * phd;
+    double * coef = V + vdoubles;
     double * acc2 = coef + (CC_F + CT::L + 1) * FS;
     int * surv = (int *)(acc2 + ((p.acc_size + 1) & ~1));   // [0, NT): FP64 list, [NT, 2 NT): FP32 list
-    const int tid = threadIdx.x;
     ColThread th;
-    col_thread<CT, NP>(th, col_pitch(FS));
+    col_thread<CT, NP>(th, col_pitch(FS), tid);
     const int role = th.role, slot = th.slot;
     const bool valid = th.valid;
     const int lane = tid & 31, warp = tid >> 5;
     long long t = 0;
-    for(long long qslot = blockIdx.x; cta_next_task(a, qslot, t, &s_qslot); qslot += gridDim.x)
+    for(long long qslot = (long long)blockIdx.x * H + grp; col_next_task(a, qslot, t, &s_qslot_g[grp], tid, sync);
+        qslot += (long long)gridDim.x * H)
     {
         int iP, iQ;
         long long off;
@@ -352,7 +395,7 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
                 wcount[0][warp] = __popc(bh);
                 wcount[1][warp] = __popc(bl);
             }
-            __syncthreads();
+            sync();
             int b0 = 0, b1 = 0;
             for(int w = 0; w < warp; w++)
             {
@@ -375,18 +418,19 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
                 s_cnt[0] = t0;
                 s_cnt[1] = t1;
             }
-            __syncthreads();
+            sync();
             const int nhi = s_cnt[0], nlo = s_cnt[1];
             if(MIXED && tid == 0 && nlo > 0 && a.fp32_count)
                 atomicAdd(a.fp32_count, (unsigned long long)nlo);
             for(int s0 = 0; s0 < nhi; s0 += FS)
-                col_block<double, CT, NP, NT>(c, surv, s0, nhi, nj, njinv, fastdiv, coef, V, FS, th, acc);
+                col_block<double, CT, NP, NT>(c, surv, s0, nhi, nj, njinv, fastdiv, coef, V, FS, th, acc, tid, sync);
             if constexpr(MIXED)
             {
                 for(int s0 = 0; s0 < nlo; s0 += FS)
-                    col_block<float, CT, NP, NT>(c, surv + NT, s0, nlo, nj, njinv, fastdiv, coef, V, FS, th, acc);
+                    col_block<float, CT, NP, NT>(c, surv + NT, s0, nlo, nj, njinv, fastdiv, coef, V, FS, th, acc, tid,
+                                                 sync);
             }
-            __syncthreads();      // surv, s_cnt and wcount are reused
+            sync();      // surv, s_cnt and wcount are reused
         }
         // sums over the batch slots, in slot order, into the accumulator
         // layout of the HRR: acc2[(g_e - lo(a)) * NTOP + t]
@@ -398,7 +442,7 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
             for(int k = 0; k < CT::NTOP; k++)
                 V[(k * NTR + (role - TOP0)) * NP + slot] = acc[k];
         }
-        __syncthreads();
+        sync();
         for(int idx = tid; idx < NTR * CT::NTOP; idx += NT)
         {
             const int k = idx / NTR, rr = idx - k * NTR;
@@ -408,7 +452,7 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
                 sum += V[(k * NTR + rr) * NP + s2];
             acc2[p.acc_off[0] + rr * p.acc_nf[0] + k] = sum;
         }
-        __syncthreads();
+        sync();
         // ---------------- HRR ----------------
         double * LA = V + p.off_hrr_b;
         double * LB = LA + p.hrr_layer;
@@ -422,16 +466,16 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
         const int nket = c2_nc(tt[2]) * c2_nc(tt[3]);
         const int accb = p.acc_off[0], accnf = p.acc_nf[0];
         const int e0 = c2_lev_off(p.elo[0]), f0 = c2_lev_off(p.flo[0]), fk = c2_lev_off(klo);
-        c2_hrr_side<NT>(p.brastep_j, p.hrr_nl[0][0], ncol, p.hrr_rows + p.hrr_base[0][0], p.hrr_loff[0][0],
+        c2_hrr_side_t<NT>(tid, sync, p.brastep_j, p.hrr_nl[0][0], ncol, p.hrr_rows + p.hrr_base[0][0], p.hrr_loff[0][0],
                         c.AB[0], c.AB[1], c.AB[2],
                         [&](int g, int col) { return acc2[accb + (g - e0) * accnf + (fk + col - f0)]; },
                         [&](int r, int col, double v) { mid[r * ncol + col] = v; }, LA, LB);
         const int kl = c2_lev_off(klo);
-        c2_hrr_side<NT>(p.ketstep_l, p.hrr_nl[0][1], nbra, p.hrr_rows + p.hrr_base[0][1], p.hrr_loff[0][1],
+        c2_hrr_side_t<NT>(tid, sync, p.ketstep_l, p.hrr_nl[0][1], nbra, p.hrr_rows + p.hrr_base[0][1], p.hrr_loff[0][1],
                         c.CD[0], c.CD[1], c.CD[2],
                         [&](int g, int row) { return mid[row * ncol + (g - kl)]; },
                         [&](int r, int row, double v) { o[oidx[row * nket + r]] = v; }, LA, LB);
-        __syncthreads();
+        sync();
     }
 }
 
@@ -439,10 +483,12 @@ k_col(const KernArgs a, const C2Params p, const int vdoubles, const int FS)
 // registry of the generated classes
 // ---------------------------------------------------------------------
 
-typedef void (*ColFn)(const KernArgs, const C2Params, const int, const int);
+typedef void (*ColFn)(const KernArgs, const C2Params, const int, const int, const int);
 
-#define COL_NNP 2
-static constexpr int COL_NPS[COL_NNP] = {4, 8};
+// variants 81, 82, 83: (primitive quartets per batch, groups per CTA)
+#define COL_NNP 3
+static constexpr int COL_NPS[COL_NNP] = {4, 8, 4};
+static constexpr int COL_HS[COL_NNP] = {1, 1, 2};
 
 struct ColKernels
 {
@@ -452,7 +498,7 @@ struct ColKernels
     int sab;                             // doubles of the stage areas SA + SB per batch slot
     int red_per_np;                      // doubles of the slot-sum scratch per batch slot
     int ncoef;                           // doubles of a coefficient record
-    int nt[COL_NNP];                     // threads per CTA for each NP
+    int nt[COL_NNP];                     // threads per group for each variant (H groups per CTA)
     ColFn fn[COL_NNP][3][2];             // [np][mode][fp64, mixed]
 };
 
@@ -466,17 +512,18 @@ template<class CT, int NPI>
 static void col_fill_np(ColKernels & k)
 {
     constexpr int NP = COL_NPS[NPI];
+    constexpr int H = COL_HS[NPI];
     k.nt[NPI] = col_nt(CT::NROLE, NP);
     for(int md = 0; md < 3; md++)
         k.fn[NPI][md][0] = k.fn[NPI][md][1] = nullptr;
-    if constexpr(col_nt(CT::NROLE, NP) <= 1024)
+    if constexpr(H * col_nt(CT::NROLE, NP) <= 1024)
     {
-        k.fn[NPI][0][0] = k_col<CT, 0, false, NP>;
-        k.fn[NPI][0][1] = k_col<CT, 0, true, NP>;
-        k.fn[NPI][1][0] = k_col<CT, 1, false, NP>;
-        k.fn[NPI][1][1] = k_col<CT, 1, true, NP>;
-        k.fn[NPI][2][0] = k_col<CT, 2, false, NP>;
-        k.fn[NPI][2][1] = k_col<CT, 2, true, NP>;
+        k.fn[NPI][0][0] = k_col<CT, 0, false, NP, H>;
+        k.fn[NPI][0][1] = k_col<CT, 0, true, NP, H>;
+        k.fn[NPI][1][0] = k_col<CT, 1, false, NP, H>;
+        k.fn[NPI][1][1] = k_col<CT, 1, true, NP, H>;
+        k.fn[NPI][2][0] = k_col<CT, 2, false, NP, H>;
+        k.fn[NPI][2][1] = k_col<CT, 2, true, NP, H>;
     }
 }
 
@@ -492,6 +539,7 @@ static void col_fill(ColKernels & k)
     k.ncoef = CC_F + CT::L + 1;
     col_fill_np<CT, 0>(k);
     col_fill_np<CT, 1>(k);
+    col_fill_np<CT, 2>(k);
 }
 
 void simint_b200_register_col(ColTable & t);

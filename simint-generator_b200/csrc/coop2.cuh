@@ -81,12 +81,18 @@ __device__ __forceinline__ int c2_index(const CartInfo * __restrict__ ci, int g,
 // x = source A | source B << 16 (function indices on layer 1, rows of the
 // previous layer after), y = direction | output row << 2 (last layer).
 // Threads form a (row, column) grid.
-template<int NT, typename IN, typename OUT>
-__device__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * __restrict__ rows,
-                            const int * loff, double X0, double X1, double X2, IN in, OUT out,
-                            double * __restrict__ LA, double * __restrict__ LB)
+struct C2SyncAll
 {
-    const int tid = threadIdx.x;
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// c2_hrr_side for NT threads numbered tid, synchronised by sync() (a CTA
+// barrier, or a named barrier of a group of NT threads).
+template<int NT, typename IN, typename OUT, typename SYNC>
+__device__ void c2_hrr_side_t(int tid, SYNC sync, int right_step, int sl_max, int ncol,
+                              const int2 * __restrict__ rows, const int * loff, double X0, double X1,
+                              double X2, IN in, OUT out, double * __restrict__ LA, double * __restrict__ LB)
+{
     const int TC = ncol < NT ? ncol : NT;
     const int TR = NT / TC;
     const int tc = tid % TC, tr = tid / TC;
@@ -102,7 +108,7 @@ __device__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * _
                 for(int col = tc; col < ncol; col += TC)
                     out(r, col, in(g, col));
             }
-        __syncthreads();
+        sync();
         return;
     }
     double * dst = LA;
@@ -140,11 +146,20 @@ __device__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * _
                     }
                 }
             }
-        __syncthreads();
+        sync();
         double * t = (double *)src;
         src = dst;
         dst = t;
     }
+}
+
+template<int NT, typename IN, typename OUT>
+__device__ __forceinline__ void c2_hrr_side(int right_step, int sl_max, int ncol, const int2 * __restrict__ rows,
+                                            const int * loff, double X0, double X1, double X2, IN in, OUT out,
+                                            double * __restrict__ LA, double * __restrict__ LB)
+{
+    c2_hrr_side_t<NT>((int)threadIdx.x, C2SyncAll(), right_step, sl_max, ncol, rows, loff, X0, X1, X2, in, out,
+                      LA, LB);
 }
 
 // 1/(2n+1), n = 0..31: the same correctly rounded values as the division,

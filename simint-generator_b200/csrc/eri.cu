@@ -1319,10 +1319,10 @@ extern "C" int simint_b200_set_variant(const int am[4], int deriv, int prec, int
         case 61: case 62: case 64: case 68:
             ok = coop2_supported(am, deriv, variant);
             break;
-        case 81: case 82:
+        case 81: case 82: case 83:
             ok = col_supported(am, deriv, variant);
             break;
-        case 181: case 182:
+        case 181: case 182: case 183:
             ok = prec == SIMINT_B200_PREC_MIXED && col_supported(am, deriv, variant - 100);
             break;
         case 121: case 122: case 124: case 128:

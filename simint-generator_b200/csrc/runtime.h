@@ -102,7 +102,8 @@ bool coop2_is_variant(int v);
 int launch_coop2(KernArgs & a, const int req[4], int deriv, int mode, int prec, cudaStream_t stream,
                  int v = 0);
 // Column kernel (colkern.cuh), deriv 0: variant codes 81 (4 primitive
-// quartets per batch) and 82 (8).
+// quartets per batch), 82 (8) and 83 (4, two groups of threads per CTA
+// running separate shell quartets).
 bool col_is_variant(int v);
 bool col_supported(const int req[4], int deriv, int v);
 int launch_col(KernArgs & a, const int req[4], int mode, int prec, cudaStream_t stream, int v);
@@ -111,9 +112,10 @@ int launch_col(KernArgs & a, const int req[4], int mode, int prec, cudaStream_t 
 // autotuner: 0 default rule, 1 straight-line, 3 cooperative v1, 4 generic,
 // 5 straight-line in FP64 even in mixed mode, 6 (7) straight-line with a
 // warp per shell quartet (in FP64 even in mixed mode), 20+B / 40+B / 60+B
-// cooperative v2 with batch B and 256 / 128 / 64 threads, 81 / 82 column
-// kernel with 4 / 8 primitive quartets per batch; 100 + a cooperative or
-// column code: that kernel in FP64 even in mixed mode.
+// cooperative v2 with batch B and 256 / 128 / 64 threads, 81 / 82 / 83
+// column kernel (4 / 8 primitive quartets per batch, 83: two groups per
+// CTA); 100 + a cooperative or column code: that kernel in FP64 even in
+// mixed mode.
 enum { VAR_DEFAULT = 0, VAR_STRAIGHT = 1, VAR_COOP2 = 2, VAR_COOP1 = 3, VAR_GENERIC = 4, VAR_STRAIGHT64 = 5,
        VAR_WARP = 6, VAR_WARP64 = 7 };
 int variant_of(const int req[4], int deriv, int prec);

@@ -861,7 +861,7 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
             if(prec == SIMINT_B200_PREC_MIXED)
                 cand.push_back(VAR_WARP64);
         }
-        for(int v : {81, 82})
+        for(int v : {81, 82, 83})
             if(col_supported(q.req, 0, v))
             {
                 cand.push_back(v);

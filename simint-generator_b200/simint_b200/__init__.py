@@ -164,6 +164,7 @@ VAR_COOP2 = {1: 21, 2: 22, 4: 24, 8: 28}          # cooperative kernel, 256 thre
 VAR_COOP2_128 = {1: 41, 2: 42, 4: 44, 8: 48}      # cooperative kernel, 128 threads, batch B
 VAR_COOP2_64 = {1: 61, 2: 62, 4: 64, 8: 68}       # cooperative kernel, 64 threads, batch B
 VAR_COL = {4: 81, 8: 82}                          # column kernel, NP primitive quartets per batch
+VAR_COL_GROUPS = 83                               # column kernel, 4 per batch, two thread groups per CTA
 
 
 def get_variant(am, deriv=0, prec=0, lib=None):

@@ -62,8 +62,8 @@ def stepdir(ijk):
             return x
 
 
-# variants: code -> primitive quartets per batch
-COL_NP = {81: 4, 82: 8}
+# variants: code -> (primitive quartets per batch, groups of threads per CTA)
+COL_NP = {81: (4, 1), 82: (8, 1), 83: (4, 2)}
 
 
 def col_supported(am):
@@ -99,11 +99,11 @@ def emit_stages(am):
     o = []
     w = o.append
     reg = lambda f, p, m: "r%d_%d_%d" % (f, p, m)
-    w("    template<typename T, int NP>")
+    w("    template<typename T, int NP, typename SYNC>")
     w("    __device__ static __forceinline__ void stages(const T * __restrict__ F0, T * __restrict__ SA,")
     w("        T * __restrict__ SB, int own, int ownF, int ostr, const int (&loff)[3], const int (&loffF)[3],")
     w("        const int (&mstrF)[3], const T (&XQ)[3], const T (&YQ)[3], T Zq, const T (&kq)[KQN],")
-    w("        const T (&cB)[3], bool valid, double (&acc)[NTOP])")
+    w("        const T (&cB)[3], bool valid, double (&acc)[NTOP], SYNC sync)")
     w("    {")
     w("        constexpr int RS = NROLE * NP;")
     # own f = 0 column, orders 0..F (from the block)
@@ -160,9 +160,9 @@ def emit_stages(am):
         w("        {")
         o.extend(body)
         w("        }")
-        w("        __syncthreads();")
+        w("        sync();")
     if F == 0:
-        w("        __syncthreads();")
+        w("        sync();")
     w("    }")
     return o
 

@@ -27,7 +27,8 @@ ERR_TIMEOUT = -6
 AM = (2, 2, 2, 2)
 
 
-@pytest.mark.parametrize("variant", [24, sb.VAR_COL[4]], ids=["cooperative", "column"])
+@pytest.mark.parametrize("variant", [24, sb.VAR_COL[4], sb.VAR_COL_GROUPS],
+                         ids=["cooperative", "column", "column_groups"])
 def test_queue_probe(variant):
     torch = pytest.importorskip("torch")
     lib = sb.load()

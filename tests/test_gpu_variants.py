@@ -2,7 +2,7 @@
 
 The autotuner may pick, per class, the register kernel, the cooperative
 kernel with 256, 128 or 64 threads and 1, 2, 4 or 8 primitive quartets per
-wavefront pass, the column kernel with 4 or 8 primitive quartets per batch,
+wavefront pass, the column kernel with 4 or 8 primitive quartets per batch (83: 4 in two thread groups per CTA),
 the first cooperative kernel or the generic kernel; each must meet the FP64
 parity bar on its own.  Variants are pinned with simint_b200_set_variant and restored
 to the default rule afterwards.
@@ -20,7 +20,7 @@ from _util import class_shells, oracle_pairs, oracle_eri, parity_bad
 pytestmark = pytest.mark.gpu
 
 VARIANTS = [sb.VAR_STRAIGHT, sb.VAR_STRAIGHT64, sb.VAR_WARP, sb.VAR_WARP64, 21, 22, 24, 28, 41, 42, 44, 48, 61, 62,
-            64, 68, sb.VAR_COL[4], sb.VAR_COL[8],
+            64, 68, sb.VAR_COL[4], sb.VAR_COL[8], sb.VAR_COL_GROUPS,
             sb.VAR_COOP1, sb.VAR_GENERIC]
 CLASSES = [(0, 0, 0, 0), (1, 0, 1, 0), (1, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 1), (2, 2, 2, 2),
            (3, 1, 2, 1), (3, 2, 1, 0), (2, 3, 3, 0), (3, 3, 2, 2), (4, 2, 1, 1), (3, 3, 3, 3)]
