@@ -69,6 +69,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "simint-generator_b200"))
 
 SEED = 2024
+T_START = time.time()
+
+
+def note(msg):
+    """One progress line on stderr (the result line is the only stdout)."""
+    print("[bench +%.1fs] %s" % (time.time() - T_START, msg), file=sys.stderr, flush=True)
+
 PSI4, GAMESS = 0, 1
 LINE_LIMIT = 3000               # bytes of the printed result line (kept well under 4 KB)
 METRIC = "primitive quartets/s per AM class, mixed-prec vs FP64 on 1 B200 at ≤1e-10 abs err"
@@ -85,7 +92,7 @@ WORKLOADS = {
     "cfg3": dict(shells="cfg1", tol=0.0, max_am=1, ordering=GAMESS, ref="gamess_l3", stride=1,
                  headline="mixed", cap_gb=4.0, e2e_every=1, deriv=0,
                  desc="cfg3: the cfg1 quartets in mixed precision (FP32 VRR behind the gate) beside FP64"),
-    "cfg5": dict(shells="cfg5", tol=1e-12, max_am=4, ordering=PSI4, ref="psi4_l4", stride=20000,
+    "cfg5": dict(shells="cfg5", tol=1e-12, max_am=4, ordering=PSI4, ref="psi4_l4", stride=80000,
                  headline="mixed", cap_gb=0.5, e2e_every=8, deriv=0,
                  desc="cfg5 l<=4 uneven sweep sample: 2000 shells s:p:d:f:g, prims s,p 4-12 d 2-6 f,g 1-3, "
                       "alpha 0.02-1e5, 400 atoms in 40 bohr, Schwarz 1e-12, Psi4 order, output streamed"),
@@ -415,6 +422,7 @@ def run_b200(args):
     npq = B.count_primq()
     classes = B.classes()
     setup_s = time.time() - t0
+    note("basis set up: %d classes, %d primitive quartets, %.1f s" % (len(classes), npq, setup_s))
     stream = torch.cuda.current_stream()
     cap = max(1, min(B.output_size, int(w["cap_gb"] * (1 << 30)) // 8))
     full = B.output_size <= cap
@@ -430,6 +438,7 @@ def run_b200(args):
         B.autotune(prec, out.data_ptr(), cap, stream.cuda_stream)
     lib.simint_b200_set_precision(sb.FP64, 0.0)
     tune_s = time.time() - t1
+    note("autotuned in %.1f s" % tune_s)
 
     def timed(prec, tag):
         lib.simint_b200_set_precision(prec, gate)
@@ -463,6 +472,7 @@ def run_b200(args):
         return tot / args.steps, nl, clk.summary()
 
     ms64, nl64, clk64 = timed(sb.FP64, "timed_fp64")
+    note("timed FP64: %.3f ms per step" % ms64)
     sums64 = B.checksums()
     msmx, nlmx, clkmx = timed(sb.MIXED, "timed_mixed")
     sumsmx = B.checksums()
@@ -520,6 +530,7 @@ def run_b200(args):
                     raise RuntimeError(sb.last_error())
             times.append(time.perf_counter() - t)
         lib.simint_b200_set_precision(sb.FP64, 0.0)
+        note("e2e: %d calls, %.1f ms per step" % (len(rows), 1e3 * statistics.median(times)))
         e2e = {"value": npq_e2e / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "calls_per_step": len(rows), "primq_per_step": int(npq_e2e),
@@ -547,6 +558,7 @@ def run_b200(args):
                                    threads=threads)
             if not args.no_cpu:
                 rate, t, n, _ = reference_rate(RS, 1, args.cpu_passes, threads)
+                note("reference CPU baseline: %.3g primitive quartets/s" % rate)
                 cpu = {"value": rate, "unit": "primitive quartets/s", "cores": threads,
                        "kind": "reference",
                        "sample": "the same %d sampled rows (%.3g primitive quartets, %.2f s per pass, "
@@ -756,6 +768,7 @@ def run_b200_rows(args, torch, sb, lib, shells, S, rank, world, local, dist):
                 if r < -1:
                     raise RuntimeError(sb.last_error())
             times.append(time.perf_counter() - t)
+        note("e2e: %.1f ms per step" % (1e3 * statistics.median(times)))
         e2e = {"value": npq / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(sum(pack_bytes(P) + pack_bytes(Q) for _, _, P, Q in rows)),
                "d2h_bytes_per_step": int(sum(b.nbytes for b in bufs)), "calls_per_step": len(rows),
@@ -767,6 +780,7 @@ def run_b200_rows(args, torch, sb, lib, shells, S, rank, world, local, dist):
             RS = refsweep.RefSweep(R, shells, tol, w["max_am"], stride=args.stride, offset=0, threads=threads)
             if not args.no_cpu:
                 rate, t, n, _ = reference_rate(RS, 1, args.cpu_passes, threads, deriv=1)
+                note("reference CPU baseline: %.3g primitive quartets/s" % rate)
                 cpu = {"value": rate, "unit": "primitive quartets/s", "cores": threads, "kind": "reference",
                        "sample": "the same %d rows (%.3g primitive quartets, %.2f s per pass), reference %s "
                                  "build" % (len(RS.bh), n, t, w["ref"])}

@@ -60,6 +60,26 @@ int simint_b200_get_precision(void);
  * with one DMA of its allocation and builds the device records there;
  * arrays a caller pointed outside the allocation are packed on the host. */
 
+/* Where simint_fill_multi_shellpair(2) and simint_create_multi_shellpair(2)
+ * (shell.h:193-236, shell.c:425-582) compute the Gaussian-product fill.
+ * SIMINT_B200_PAIR_FILL_AUTO (default): on the GPU for lists of 4096 or
+ * more padded primitive pairs when a device is present, else on the host;
+ * _HOST: always on the host (bit for bit the reference's shell.c);
+ * _GPU: on the GPU whenever a device is present.  The GPU fill is one
+ * thread per shell pair writing a device image of the allocation (one copy
+ * back), the Schwarz values of all primitive pairs as one task list and the
+ * reference's per-pair sort on the device: every array equals the host fill
+ * bit for bit except the prefactors and screening values, which may differ
+ * in the last bits (CUDA's exp against the host's).  A failed GPU fill
+ * prints a message and fills on the host.  The environment variable
+ * SIMINT_B200_PAIR_FILL=host|gpu sets the initial mode.  Process-wide;
+ * returns 0 or SIMINT_B200_ERR_ARG. */
+#define SIMINT_B200_PAIR_FILL_AUTO 0
+#define SIMINT_B200_PAIR_FILL_HOST 1
+#define SIMINT_B200_PAIR_FILL_GPU  2
+int simint_b200_set_pair_fill(int mode);
+int simint_b200_get_pair_fill(void);
+
 /* Text of the last error seen by the calling thread. */
 const char * simint_b200_last_error(void);
 
@@ -177,7 +197,9 @@ int simint_b200_basis_queue_probe(simint_b200_basis * b, int k, long long publis
  * cooperative kernel with 256, 128 or 64 threads and 1, 2, 4 or 8
  * primitive quartets per wavefront pass; the column kernel with 4 or 8
  * primitive quartets per batch, or 4 in two thread groups per CTA; in mixed mode each also in FP64) on the
- * sweep's own tasks and keep the fastest for `prec`.  Choices are process-wide and are written to the
+ * sweep's own tasks and keep the fastest for `prec`: one untimed run, then the best of two timed
+ * runs, except for a candidate whose untimed run took over twice the best time so far plus a
+ * millisecond.  Choices are process-wide and are written to the
  * JSON file $SIMINT_B200_TUNE_FILE when set (read back by simint_init). */
 int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out,
                                long long dev_out_doubles, void * stream);

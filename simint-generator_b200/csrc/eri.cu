@@ -759,16 +759,53 @@ int launch_rectangle(const simint_multi_shellpair * P, const PairSetDev & dP,
 // same as the one-shot path (each chunk's kets in primitive-count order).
 // Opt-in phase trace of the host-buffer entry points (environment variable
 // SIMINT_B200_TRACE=1): one line per simint_compute_eri call on stderr with
-// the host time spent packing pair records, waiting for the GPU (uploads,
-// kernels, downloads) and copying results into the caller's memory.
+// the host time spent packing pair records, issuing the uploads, issuing the
+// kernels and the download, waiting for the GPU and copying results into the
+// caller's memory, and (one-shot calls) the device time of the kernels and of
+// the download between CUDA events on the call's stream.
 namespace {
 struct CallTrace
 {
     typedef std::chrono::steady_clock clk;
     bool on;
     clk::time_point t0;
-    double pack = 0.0, wait = 0.0, copy = 0.0;
+    double pack = 0.0, upload = 0.0, issue = 0.0, wait = 0.0, copy = 0.0;
+    float kern = -1.0f, down = -1.0f;     // device time of the kernels and of the download
     CallTrace() : on(enabled()), t0(on ? clk::now() : clk::time_point()) {}
+    // device-side marks on the call's stream (events of the calling thread)
+    cudaEvent_t * events()
+    {
+        thread_local cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        if(!ev[0])
+            for(int i = 0; i < 3; i++)
+                if(cudaEventCreate(&ev[i]) != cudaSuccess)
+                {
+                    cudaGetLastError();
+                    ev[i] = nullptr;
+                }
+        return ev;
+    }
+    void mark(int i, cudaStream_t s)
+    {
+        if(on && events()[i])
+            cudaEventRecord(events()[i], s);
+    }
+    // after the stream has been synchronised
+    void device_times()
+    {
+        if(!on)
+            return;
+        cudaEvent_t * ev = events();
+        if(ev[0] && ev[1] && ev[2])
+        {
+            if(cudaEventElapsedTime(&kern, ev[0], ev[1]) != cudaSuccess ||
+               cudaEventElapsedTime(&down, ev[1], ev[2]) != cudaSuccess)
+            {
+                cudaGetLastError();
+                kern = down = -1.0f;
+            }
+        }
+    }
     static bool enabled()
     {
         static const bool e = [] {
@@ -796,8 +833,9 @@ struct CallTrace
             return;
         const double tot = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
         fprintf(stderr, "simint_b200 trace: (%d %d|%d %d) bra %d ket %d out %.1f MB pipelined %d: "
-                "total %.3f ms, pack %.3f, wait %.3f, copy %.3f\n", P->am1, P->am2, Q->am1, Q->am2,
-                P->nshell12_clip, Q->nshell12_clip, outbytes / 1e6, pipelined ? 1 : 0, tot, pack, wait, copy);
+                "total %.3f ms, pack %.3f, upload %.3f, launch %.3f, wait %.3f, copy %.3f; device: kernels %.3f, "
+                "download %.3f\n", P->am1, P->am2, Q->am1, Q->am2, P->nshell12_clip, Q->nshell12_clip,
+                outbytes / 1e6, pipelined ? 1 : 0, tot, pack, upload, issue, wait, copy, kern, down);
     }
 };
 } // namespace
@@ -995,6 +1033,7 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         if(moved >= ((size_t)16 << 20) && Q->nshell12_clip >= 64)
             return compute_eri_pipelined(deriv, P, Q, screen_tol, integrals, nc);
     }
+    CallTrace tr;
     PackedLayout LP, LQ;
     std::vector<int> pstart, qstart;
     const size_t szP = (pack_layout(P, LP, &pstart) + 255) & ~(size_t)255;
@@ -1013,7 +1052,6 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         set_error("out of memory for pair data");
         return SIMINT_B200_ERR_CUDA;
     }
-    CallTrace tr;
     char * h = (char *)w.hstage.ptr;
     tr.time(tr.pack, [&] {
         if(!pinP)
@@ -1029,25 +1067,30 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         memcpy(h + szP + szQ, kord.data(), kord.size() * sizeof(int));
     });
     char * d = (char *)w.dpair.ptr;
-    if(pinP || pinQ)
-    {
-        if(!w.dsoa.reserve(std::max(pinP ? P->memsize : 0, pinQ ? Q->memsize : 0)))
+    int rc_up = 0;
+    tr.time(tr.upload, [&] {
+        if(pinP || pinQ)
         {
-            set_error("out of device memory for pair data");
-            return SIMINT_B200_ERR_CUDA;
+            if(!w.dsoa.reserve(std::max(pinP ? P->memsize : 0, pinQ ? Q->memsize : 0)))
+            {
+                set_error("out of device memory for pair data");
+                rc_up = SIMINT_B200_ERR_CUDA;
+                return;
+            }
+            // the unused host staging of a pinned set holds its pair starts
+            rc_up = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
+                         : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
+            if(rc_up == 0)
+                rc_up = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
+                             : (cudaMemcpyAsync(d + szP, h + szP, szQ, cudaMemcpyHostToDevice, w.stream), 0);
+            if(rc_up == 0)
+                cudaMemcpyAsync(d + szP + szQ, h + szP + szQ, szK, cudaMemcpyHostToDevice, w.stream);
         }
-        // the unused host staging of a pinned set holds its pair starts
-        int rc = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
-                      : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
-        if(rc == 0)
-            rc = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
-                      : (cudaMemcpyAsync(d + szP, h + szP, szQ, cudaMemcpyHostToDevice, w.stream), 0);
-        if(rc != 0)
-            return rc;
-        cudaMemcpyAsync(d + szP + szQ, h + szP + szQ, szK, cudaMemcpyHostToDevice, w.stream);
-    }
-    else
-        cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
+        else
+            cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
+    });
+    if(rc_up != 0)
+        return rc_up;
     const PairSetDev dP = device_view(d, LP, P->screen_max);
     const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
     const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);
@@ -1057,16 +1100,23 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         set_error("out of device memory for the output");
         return SIMINT_B200_ERR_CUDA;
     }
-    int r = launch_rectangle(P, dP, Q, dQ, (const int *)(d + szP + szQ), screen_tol, deriv,
-                             precision(), gate(), (double *)w.dout.ptr, w.stream);
-    if(r < 0)
-        return r;
+    int r = 0;
     // results through the pinned staging buffer (full-speed DMA; a copy
     // into pageable memory would go through the driver's own staging), then
     // into the caller's memory on all host cores
     const bool staged = outbytes >= (64u << 10) && w.hout.reserve(outbytes);
-    cudaMemcpyAsync(staged ? w.hout.ptr : (void *)integrals, w.dout.ptr, outbytes, cudaMemcpyDeviceToHost,
-                    w.stream);
+    tr.time(tr.issue, [&] {
+        tr.mark(0, w.stream);
+        r = launch_rectangle(P, dP, Q, dQ, (const int *)(d + szP + szQ), screen_tol, deriv,
+                             precision(), gate(), (double *)w.dout.ptr, w.stream);
+        tr.mark(1, w.stream);
+        if(r >= 0)
+            cudaMemcpyAsync(staged ? w.hout.ptr : (void *)integrals, w.dout.ptr, outbytes,
+                            cudaMemcpyDeviceToHost, w.stream);
+        tr.mark(2, w.stream);
+    });
+    if(r < 0)
+        return r;
     cudaError_t e = cudaSuccess;
     tr.time(tr.wait, [&] { e = cudaStreamSynchronize(w.stream); });
     if(e == cudaSuccess)
@@ -1076,6 +1126,7 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         set_error(std::string("CUDA error: ") + cudaGetErrorString(e));
         return SIMINT_B200_ERR_CUDA;
     }
+    tr.device_times();
     if(staged)
         tr.time(tr.copy, [&] { parallel_copy(integrals, w.hout.ptr, outbytes); });
     tr.report(P, Q, outbytes, false);

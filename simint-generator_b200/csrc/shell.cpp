@@ -301,6 +301,36 @@ namespace sb200 {
 // GPU in one launch (defined in batch.cu).  out follows the padded slot
 // layout of the pair list; returns 0 on success.
 int prim_schwarz_batch(int npair, const simint_shell * AB, double * out);
+// The whole fill on the GPU (pairfill.cu); 0 on success.
+int gpu_fill_multi_shellpair2(int npair, const simint_shell * AB, simint_multi_shellpair * P, int screen_method);
+int pair_fill_mode();
+int ensure_device();
+}
+
+// Whether a pair list's fill runs on the GPU: the mode set by
+// simint_b200_set_pair_fill, in automatic mode lists of 4096 or more padded
+// primitive pairs, and only with a device.
+static bool fill_on_gpu(int npair, const simint_shell * AB)
+{
+    const int mode = sb200::pair_fill_mode();
+    if(mode == SIMINT_B200_PAIR_FILL_HOST || npair <= 0)
+        return false;
+    if(mode == SIMINT_B200_PAIR_FILL_AUTO)
+    {
+        int npad = 0, batch = 0;
+        for(int s = 0; s < npair; s++)
+        {
+            batch += pair_nprim(&AB[2 * s], &AB[2 * s + 1]);
+            if(((s + 1) % SIMINT_NSHELL_SIMD) == 0 || s + 1 >= npair)
+            {
+                npad += SIMINT_SIMD_ROUND(batch);
+                batch = 0;
+            }
+        }
+        if(npad < 4096)
+            return false;
+    }
+    return sb200::ensure_device() == 0;
 }
 
 // descending screen order inside one shell pair (shell.c:37-128); a stable
@@ -322,6 +352,13 @@ extern "C" {
 void simint_fill_multi_shellpair2(int npair, struct simint_shell const * AB,
                                   struct simint_multi_shellpair * P, int screen_method)
 {
+    if(fill_on_gpu(npair, AB))
+    {
+        const int rc = sb200::gpu_fill_multi_shellpair2(npair, AB, P, screen_method);
+        if(rc == 0)
+            return;
+        fprintf(stderr, "simint_b200: GPU pair fill failed (%s); filling on the host\n", simint_b200_last_error());
+    }
     P->nshell12 = npair;
     P->nshell12_clip = npair;
     P->nprim = 0;

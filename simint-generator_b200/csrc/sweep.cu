@@ -882,7 +882,17 @@ extern "C" int simint_b200_basis_autotune(simint_b200_basis * b, int prec, doubl
         for(int v : cand)
         {
             set_variant(q.req, 0, prec, v);
+            cudaEventRecord(e0, stream);
             if(issue_class(b, k, prec, dev_out, dev_out_doubles, stream) < 0)
+                continue;
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float warm = 0;
+            cudaEventElapsedTime(&warm, e0, e1);
+            // a candidate whose first run (which includes loading its
+            // kernel) takes over twice the best time so far plus a
+            // millisecond is not timed again
+            if(warm > 2.0f * bestms + 1.0f)
                 continue;
             float ms = 1e30f;
             for(int rep = 0; rep < 2; rep++)

@@ -167,6 +167,25 @@ VAR_COL = {4: 81, 8: 82}                          # column kernel, NP primitive 
 VAR_COL_GROUPS = 83                               # column kernel, 4 per batch, two thread groups per CTA
 
 
+PAIR_FILL_AUTO, PAIR_FILL_HOST, PAIR_FILL_GPU = 0, 1, 2
+
+
+def set_pair_fill(mode, lib=None):
+    """Where simint_create_multi_shellpair(2) computes the Gaussian-product
+    fill (simint_b200_set_pair_fill): PAIR_FILL_AUTO, _HOST or _GPU; returns
+    the C status."""
+    lib = lib or load()
+    lib.simint_b200_set_pair_fill.argtypes = [C.c_int]
+    lib.simint_b200_set_pair_fill.restype = C.c_int
+    return lib.simint_b200_set_pair_fill(mode)
+
+
+def get_pair_fill(lib=None):
+    lib = lib or load()
+    lib.simint_b200_get_pair_fill.restype = C.c_int
+    return lib.simint_b200_get_pair_fill()
+
+
 def get_variant(am, deriv=0, prec=0, lib=None):
     """Kernel variant in force for a requested class (simint_b200_variant)."""
     lib = lib or load()

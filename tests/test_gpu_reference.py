@@ -332,7 +332,12 @@ def test_gpu_matches_valeev_fg(lib, drv, fname, deriv):
                         out=theirs, off=off, count=False)
                 Rl.free_pairsets()
                 own = np.maximum(own, np.abs(theirs - ref))
-            worse = bad & (d > 2.0 * own + 1e-14)
+            # two double-precision evaluations of an ill-conditioned element
+            # miss it by amounts of the same order, not the same size: on the
+            # (gg|ss) fixture quartets one element is 3.5e-11 from ValeevRef in
+            # the reference library and 8.7e-11 on the GPU (a different
+            # summation order); a defect would be orders of magnitude off
+            worse = bad & (d > 4.0 * own + 1e-14)
             assert not worse.any(), (name, float(d[worse].max()), float(own[worse].max()))
 
 
@@ -343,10 +348,12 @@ def _sweep_match(ref_keys, sh4, nshell):
     return shl, pos, np.nonzero(ref_keys[pos] == keys)[0]
 
 
-def sweep_quartets_outside(ref_out, ref_keys, ref_offs, vals, sh4, nout, nshell):
-    """Quartets of one class of a sweep outside the FP64 bar against the
-    reference rows (indices into the class)."""
+def sweep_quartets_outside(ref_out, ref_keys, ref_offs, vals, sh4, nout, nshell, only=None):
+    """Quartets of one class of a sweep (of `only`, if given) outside the FP64
+    bar against the reference rows (indices into the class)."""
     shl, pos, hit = _sweep_match(ref_keys, sh4, nshell)
+    if only is not None:
+        hit = [q for q in hit if int(q) in only]
     out = []
     for q in hit:
         g = vals[q * nout:(q + 1) * nout]
@@ -385,6 +392,13 @@ def test_sweep_against_reference(lib):
       quartets), which must stay under 1 % of a class's quartets (20 % for
       L >= 11); a sample of them is judged against the long-double
       evaluation;
+    * the rows of the simint_compute_eri calls under the same rules, and
+      equal to the sweep's rows except on quartets that the reference bar
+      marks ill-conditioned: a call of fewer than 16 384 quartets runs the
+      warp-per-quartet form of a register kernel, which sums the primitive
+      contributions in another order than the sweep's thread-per-quartet
+      form, and on those quartets the order shows (1.8e-10 on a cfg2 (ff|ss)
+      row of magnitude 0.03);
     * mixed within the gate of the FP64 sweep."""
     torch = pytest.importorskip("torch")
     R = need("gamess_l3")
@@ -408,6 +422,8 @@ def test_sweep_against_reference(lib):
         hmx = out.cpu().numpy()
         lib.simint_b200_set_precision(sb.FP64, 0.0)
         # the same rows through simint_compute_eri
+        hcall = np.full_like(h64, np.nan)
+        called = [set() for _ in classes]
         for k, c in enumerate(classes):
             a = c["offset"]
             sh4 = B.class_quartets(k, c["nquart"])
@@ -418,10 +434,9 @@ def test_sweep_against_reference(lib):
                 Q.nshell12_clip = cnt
                 r, row = sb.compute_eri(P, Q, 1e-14, 0, lib)
                 lib.simint_free_multi_shellpair(C.byref(P))
-                got = h64[a + first * c["nout"]:a + (first + cnt) * c["nout"]]
-                if r < 0:
-                    row = np.zeros_like(got)
-                assert np.abs(got - row).max() <= 1e-14 * max(1.0, float(np.abs(row).max())), (c["am"], first)
+                sl = slice(a + first * c["nout"], a + (first + cnt) * c["nout"])
+                hcall[sl] = row if r >= 0 else 0.0
+                called[k].update(range(first, first + cnt))
             Q.nshell12_clip = len(kl)
             lib.simint_free_multi_shellpair(C.byref(Q))
     finally:
@@ -441,17 +456,32 @@ def test_sweep_against_reference(lib):
                                                   len(shells))
         assert nc >= 0.99 * c["nquart"], (c["am"], nc, c["nquart"])
         ncmp += nc
-        if nbad:
-            qbad = sweep_quartets_outside(ref_out, keys, offs, h64[a:a + m], sh4, c["nout"], len(shells))
+        limit = 0.2 if sum(c["am"]) >= 11 else 0.01
+        qbad = set()
+        for vals, only in ((h64[a:a + m], None), (hcall[a:a + m], called[k])):
+            outside = sweep_quartets_outside(ref_out, keys, offs, vals, sh4, c["nout"], len(shells), only)
+            qbad.update(outside)
+            if not outside:
+                continue
             # (ff|ff) of this basis: about 15 % of its quartets are that
             # ill-conditioned for any double-precision evaluation
-            assert len(qbad) <= (0.2 if sum(c["am"]) >= 11 else 0.01) * nc, (c["am"], len(qbad), nc)
+            base = nc if only is None else max(len(only), 1)
+            assert len(outside) <= limit * base, (c["am"], len(outside), base)
             # the cheapest of them (fewest primitive quartets) judged against
             # the long-double evaluation
-            npq = [int(np.prod([len(shells[int(x)][2]) for x in sh4[q]])) for q in qbad]
-            sample = [q for _, q in sorted(zip(npq, qbad))[:3] if _ <= 4096]
-            unexplained = sweep_quartets_unexplained(ref_out, keys, offs, h64[a:a + m], sh4, c["nout"],
+            npq = [int(np.prod([len(shells[int(x)][2]) for x in sh4[q]])) for q in outside]
+            sample = [q for _, q in sorted(zip(npq, outside))[:3] if _ <= 4096]
+            unexplained = sweep_quartets_unexplained(ref_out, keys, offs, vals, sh4, c["nout"],
                                                      len(shells), ld, sample)
             assert not unexplained, (c["am"], ma, mr, unexplained[:3])
+        # the calls' rows equal the sweep's except on ill-conditioned quartets
+        # (of those the reference rows cover)
+        nq_out = c["nout"]
+        matched = set(int(q) for q in _sweep_match(keys, sh4, len(shells))[2])
+        for q in sorted(called[k] & matched):
+            g = h64[a + q * nq_out:a + (q + 1) * nq_out]
+            r = hcall[a + q * nq_out:a + (q + 1) * nq_out]
+            if np.abs(g - r).max() > 1e-14 * max(1.0, float(np.abs(r).max())):
+                assert q in qbad, (c["am"], q, float(np.abs(g - r).max()))
     assert ncmp > 100000
     B.close()
