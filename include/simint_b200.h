@@ -335,6 +335,21 @@ int simint_b200_basis_nbf(simint_b200_basis const * b);
 int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
                          const double * dev_D, double * dev_J, double * dev_K, void * stream);
 
+/* The sweep and its J/K digestion in one pass, without the sweep's output
+ * in HBM: each class runs in chunks of scratch_doubles / (integrals per
+ * quartet) shell quartets through dev_scratch, and each chunk is contracted
+ * into J and K (as simint_b200_basis_jk) right after it is computed, on the
+ * same stream, while its integrals are still in the 126 MB L2 (a scratch
+ * buffer of a few tens of MB keeps them there).  prec as for
+ * simint_b200_basis_compute; the class checksums are accumulated as by a
+ * streamed compute.  dev_scratch must hold one quartet of every class;
+ * classes whose digestion does not fit shared memory return
+ * SIMINT_B200_ERR_CLASS.  Issued eagerly on `stream`; returns the number of
+ * kernel launches or a negative SIMINT_B200_ERR_*. */
+int simint_b200_basis_compute_jk(simint_b200_basis * b, int prec, const double * dev_D, double * dev_J,
+                                 double * dev_K, double * dev_scratch, long long scratch_doubles,
+                                 void * stream);
+
 /* One-electron matrices of a whole basis (the batched form of
  * simint_compute_overlap / simint_compute_ke / simint_compute_potential,
  * skel/simint/simint_oneelectron.h:12-27): kind SIMINT_B200_OEI_OVERLAP,

@@ -705,8 +705,19 @@ static unsigned long long * class_fp32(simint_b200_basis * b, size_t k)
 #define SWEEP_SPIN_LIMIT 1000000ull
 
 // Issue the launches of class k (ERI chunks + checksums) on `stream`.
+// J/K digestion of a streamed sweep (simint_b200_basis_compute_jk): each
+// chunk of a class's integrals is contracted right after it is computed,
+// while it is still in L2.
+struct JKJob
+{
+    const double * D;
+    double *J, *K;
+};
+static int jk_chunk(simint_b200_basis * b, size_t k, const double * out, long long t0, long long cn,
+                    const JKJob & job, cudaStream_t stream);
+
 static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout, long long cap,
-                       cudaStream_t stream)
+                       cudaStream_t stream, const JKJob * jk = nullptr)
 {
     int nl = 0;
     const bool full = cap >= b->total_out;
@@ -750,6 +761,13 @@ static int issue_class(simint_b200_basis * b, size_t k, int prec, double * dout,
         k_checksum<<<blocks, 256, 0, stream>>>(a.out, n, dsums + 2 * k);
         count_launch(1);
         nl++;
+        if(jk)
+        {
+            rc = jk_chunk(b, k, a.out, t0, cn, *jk, stream);
+            if(rc < 0)
+                return rc;
+            nl += rc;
+        }
     }
     return nl;
 }
@@ -1147,7 +1165,8 @@ struct JKArgs
     const int * aooff;
     int na, nbb, nc, nd;
     int same_class;                 // bra and ket pair classes equal (unique pair-pairs)
-    const double * out;
+    const double * out;             // integrals of tasks task0 .. task0 + ntask - 1
+    long long task0;
     const double * D;
     double * J, * K;
     int nbf;
@@ -1287,7 +1306,7 @@ __global__ void __launch_bounds__(32 * WPB) k_jk(const JKArgs g)
         return;
     int2 ab, cd;
     double sc;
-    jk_quartet(g, t, ab, cd, sc);
+    jk_quartet(g, g.task0 + t, ab, cd, sc);
     const int nout = g.na * g.nbb * g.nc * g.nd;
     double * I = jsm + (size_t)warp * (nout + jk_dsize(g.na, g.nbb, g.nc, g.nd));
     double * Ds = I + nout;
@@ -1309,7 +1328,7 @@ __global__ void __launch_bounds__(NT) k_jkb(const JKArgs g)
     const long long t = blockIdx.x;
     int2 ab, cd;
     double sc;
-    jk_quartet(g, t, ab, cd, sc);
+    jk_quartet(g, g.task0 + t, ab, cd, sc);
     const int nout = g.na * g.nbb * g.nc * g.nd;
     double * Ds = jsm + nout;
     const double * src = g.out + t * (long long)nout;
@@ -1346,16 +1365,10 @@ extern "C" int simint_b200_basis_nbf(simint_b200_basis const * b)
     return n;
 }
 
-extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
-                                    const double * dev_D, double * dev_J, double * dev_K, void * stream_)
+// Shell offsets and pair shell lists of the digestion (once per basis);
+// every shell must take part in the sweep (none above its max_am).
+static int jk_prepare(simint_b200_basis * b)
 {
-    if(!b || !dev_out || !dev_D || !dev_J || !dev_K || dev_out_doubles < b->total_out)
-    {
-        set_error("simint_b200_basis_jk needs the full-layout output of the sweep");
-        return SIMINT_B200_ERR_ARG;
-    }
-    cudaStream_t stream = (cudaStream_t)stream_;
-    const int nbf = simint_b200_basis_nbf(b);
     if(!b->daooff.ptr)
     {
         std::vector<int> off(b->shells.size());
@@ -1377,9 +1390,8 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
                 return SIMINT_B200_ERR_CUDA;
             cudaMemcpy(pc.dsh.ptr, sh.data(), sh.size() * sizeof(int2), cudaMemcpyHostToDevice);
         }
-        b->nbf = nbf;
+        b->nbf = simint_b200_basis_nbf(b);
     }
-    // every shell must take part in the sweep (none above its max_am)
     for(const auto & sh : b->shells)
     {
         bool found = false;
@@ -1392,61 +1404,158 @@ extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_ou
             return SIMINT_B200_ERR_ARG;
         }
     }
-    cudaMemsetAsync(dev_J, 0, (size_t)nbf * nbf * sizeof(double), stream);
-    cudaMemsetAsync(dev_K, 0, (size_t)nbf * nbf * sizeof(double), stream);
-    int nl = 0;
-    for(auto & q : b->qcs)
+    return 0;
+}
+
+// Shared memory of the digestion of one quartet of class q (integrals and
+// density blocks), or 0 when it exceeds 227 KB.
+static size_t jk_quartet_bytes(const QClass & q)
+{
+    const size_t per = ((size_t)q.nout + jk_dsize(ncart_of(q.req[0]), ncart_of(q.req[1]), ncart_of(q.req[2]),
+                                                   ncart_of(q.req[3]))) * sizeof(double);
+    return per > 227 * 1024 ? 0 : per;
+}
+
+// Contract tasks t0 .. t0 + cn - 1 of class k, whose integrals are at out,
+// into the raw J and K sums.  Returns the launches (1) or an error.
+static int jk_launch(simint_b200_basis * b, size_t k, const double * out, long long t0, long long cn,
+                     const JKJob & job, cudaStream_t stream)
+{
+    const QClass & q = b->qcs[k];
+    KernArgs a;
+    fill_args(b, q, a);
+    JKArgs g;
+    g.prefix = a.prefix;
+    g.border = a.border;
+    g.korder = a.korder;
+    g.nb = a.nb;
+    g.ntask = cn;
+    g.task0 = t0;
+    g.shX = (const int2 *)b->pcs[q.bx].dsh.ptr;
+    g.shY = (const int2 *)b->pcs[q.ky].dsh.ptr;
+    g.aooff = (const int *)b->daooff.ptr;
+    g.na = ncart_of(q.req[0]); g.nbb = ncart_of(q.req[1]); g.nc = ncart_of(q.req[2]); g.nd = ncart_of(q.req[3]);
+    g.same_class = q.bx == q.ky;
+    g.out = out;
+    g.D = job.D;
+    g.J = job.J;
+    g.K = job.K;
+    g.nbf = b->nbf;
+    // the quartet's integrals and density blocks are staged in shared
+    // memory: one quartet per warp, 4 warps per block, while they fit
+    // 96 KB; else one quartet per 256-thread block, up to 227 KB (about
+    // 28 000 integrals per shell quartet: (gg|gd), (gf|gf), (gg|ff))
+    const size_t per_warp = jk_quartet_bytes(q);
+    if(!per_warp)
     {
-        if(q.ntask == 0)
-            continue;
-        KernArgs a;
-        fill_args(b, q, a);
-        JKArgs g;
-        g.prefix = a.prefix;
-        g.border = a.border;
-        g.korder = a.korder;
-        g.nb = a.nb;
-        g.ntask = q.ntask;
-        g.shX = (const int2 *)b->pcs[q.bx].dsh.ptr;
-        g.shY = (const int2 *)b->pcs[q.ky].dsh.ptr;
-        g.aooff = (const int *)b->daooff.ptr;
-        g.na = ncart_of(q.req[0]); g.nbb = ncart_of(q.req[1]); g.nc = ncart_of(q.req[2]); g.nd = ncart_of(q.req[3]);
-        g.same_class = q.bx == q.ky;
-        g.out = dev_out + q.offset;
-        g.D = dev_D;
-        g.J = dev_J;
-        g.K = dev_K;
-        g.nbf = nbf;
-        // the quartet's integrals and density blocks are staged in shared
-        // memory: one quartet per warp, 4 warps per block, while they fit
-        // 96 KB; else one quartet per 256-thread block, up to 227 KB (about
-        // 28 000 integrals per shell quartet: (gg|gd), (gf|gf), (gg|ff))
-        const size_t per_warp = ((size_t)q.nout + jk_dsize(g.na, g.nbb, g.nc, g.nd)) * sizeof(double);
-        if(per_warp > 227 * 1024)
-        {
-            set_error("simint_b200_basis_jk: class too large for the digestion kernel");
-            return SIMINT_B200_ERR_CLASS;
-        }
-        if(4 * per_warp <= 96 * 1024)
-        {
-            cudaFuncSetAttribute(k_jk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-            k_jk<4><<<(unsigned)((q.ntask + 3) / 4), 128, 4 * per_warp, stream>>>(g);
-        }
-        else
-        {
-            cudaFuncSetAttribute(k_jkb<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-            k_jkb<256><<<(unsigned)q.ntask, 256, per_warp, stream>>>(g);
-        }
-        nl++;
+        set_error("J/K digestion: class too large for the digestion kernel");
+        return SIMINT_B200_ERR_CLASS;
     }
-    const long long nn = (long long)nbf * nbf;
-    k_jk_sym<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(dev_J, dev_K, nbf);
-    count_launch(nl + 1);
+    if(4 * per_warp <= 96 * 1024)
+    {
+        cudaFuncSetAttribute(k_jk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        k_jk<4><<<(unsigned)((cn + 3) / 4), 128, 4 * per_warp, stream>>>(g);
+    }
+    else
+    {
+        cudaFuncSetAttribute(k_jkb<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        k_jkb<256><<<(unsigned)cn, 256, per_warp, stream>>>(g);
+    }
+    count_launch(1);
+    return 1;
+}
+
+static int jk_chunk(simint_b200_basis * b, size_t k, const double * out, long long t0, long long cn,
+                    const JKJob & job, cudaStream_t stream)
+{
+    return jk_launch(b, k, out, t0, cn, job, stream);
+}
+
+static int jk_finish(simint_b200_basis * b, const JKJob & job, cudaStream_t stream)
+{
+    const long long nn = (long long)b->nbf * b->nbf;
+    k_jk_sym<<<(unsigned)((nn + 255) / 256), 256, 0, stream>>>(job.J, job.K, b->nbf);
+    count_launch(1);
     const cudaError_t e = cudaGetLastError();
     if(e != cudaSuccess)
     {
-        set_error(std::string("simint_b200_basis_jk: ") + cudaGetErrorString(e));
+        set_error(std::string("J/K digestion: ") + cudaGetErrorString(e));
         return SIMINT_B200_ERR_CUDA;
     }
-    return nl + 1;
+    return 1;
+}
+
+extern "C" int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long long dev_out_doubles,
+                                    const double * dev_D, double * dev_J, double * dev_K, void * stream_)
+{
+    if(!b || !dev_out || !dev_D || !dev_J || !dev_K || dev_out_doubles < b->total_out)
+    {
+        set_error("simint_b200_basis_jk needs the full-layout output of the sweep");
+        return SIMINT_B200_ERR_ARG;
+    }
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int rc = jk_prepare(b);
+    if(rc < 0)
+        return rc;
+    const int nbf = b->nbf;
+    cudaMemsetAsync(dev_J, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    cudaMemsetAsync(dev_K, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    const JKJob job = {dev_D, dev_J, dev_K};
+    int nl = 0;
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        const QClass & q = b->qcs[k];
+        if(q.ntask == 0)
+            continue;
+        rc = jk_launch(b, k, dev_out + q.offset, 0, q.ntask, job, stream);
+        if(rc < 0)
+            return rc;
+        nl += rc;
+    }
+    rc = jk_finish(b, job, stream);
+    return rc < 0 ? rc : nl + rc;
+}
+
+extern "C" int simint_b200_basis_compute_jk(simint_b200_basis * b, int prec, const double * dev_D,
+                                            double * dev_J, double * dev_K, double * dev_scratch,
+                                            long long scratch_doubles, void * stream_)
+{
+    if(!b || !dev_D || !dev_J || !dev_K || !dev_scratch || scratch_doubles <= 0)
+    {
+        set_error("bad argument to simint_b200_basis_compute_jk");
+        return SIMINT_B200_ERR_ARG;
+    }
+    if(prec != SIMINT_B200_PREC_FP64 && prec != SIMINT_B200_PREC_MIXED)
+        return SIMINT_B200_ERR_ARG;
+    for(const auto & q : b->qcs)
+        if(q.ntask > 0 && (scratch_doubles < q.nout || !jk_quartet_bytes(q)))
+        {
+            set_error(scratch_doubles < q.nout ? "scratch buffer smaller than one quartet of a class"
+                                               : "J/K digestion: class too large for the digestion kernel");
+            return scratch_doubles < q.nout ? SIMINT_B200_ERR_ARG : SIMINT_B200_ERR_CLASS;
+        }
+    cudaStream_t stream = (cudaStream_t)stream_;
+    int rc = jk_prepare(b);
+    if(rc < 0)
+        return rc;
+    const int nbf = b->nbf;
+    cudaMemsetAsync(dev_J, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    cudaMemsetAsync(dev_K, 0, (size_t)nbf * nbf * sizeof(double), stream);
+    cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
+    cudaMemsetAsync(b->dqueue.ptr, 0, SWEEP_QSTRIDE * b->qcs.size(), stream);
+    const JKJob job = {dev_D, dev_J, dev_K};
+    // a scratch buffer that holds the whole sweep is used as such: each
+    // class writes its own range and is digested from there
+    int nl = 0;
+    for(size_t k = 0; k < b->qcs.size(); k++)
+    {
+        if(b->qcs[k].ntask == 0)
+            continue;
+        rc = issue_class(b, k, prec, dev_scratch, scratch_doubles, stream, &job);
+        if(rc < 0)
+            return rc;
+        nl += rc;
+    }
+    rc = jk_finish(b, job, stream);
+    return rc < 0 ? rc : nl + rc;
 }

@@ -393,6 +393,19 @@ class Basis:
             raise RuntimeError("simint_b200_basis_jk failed: " + last_error())
         return r
 
+    def compute_jk(self, prec, dev_D, dev_J, dev_K, dev_scratch, scratch_doubles, stream=0):
+        """The sweep and its J/K digestion chunk by chunk through a scratch
+        buffer (simint_b200_basis_compute_jk); device pointers."""
+        L = self.lib
+        L.simint_b200_basis_compute_jk.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                   C.c_void_p, C.c_longlong, C.c_void_p]
+        r = L.simint_b200_basis_compute_jk(self.h, prec, C.c_void_p(dev_D), C.c_void_p(dev_J),
+                                           C.c_void_p(dev_K), C.c_void_p(dev_scratch), scratch_doubles,
+                                           C.c_void_p(stream))
+        if r < 0:
+            raise RuntimeError("simint_b200_basis_compute_jk failed: " + last_error())
+        return r
+
     def class_times(self, prec, dev_ptr, ndoubles, stream=0):
         n = self.lib.simint_b200_basis_nclass(self.h)
         ms = (C.c_float * max(n, 1))()

@@ -1,12 +1,14 @@
 """Micro-benchmarks of the integral consumers next to the ERI sweep.
 
-    python -m simint_b200.auxbench jk  [--stride 8000] [--reps 5]
+    python -m simint_b200.auxbench jk  [--stride 8000] [--reps 5] [--scratch-mb 48]
     python -m simint_b200.auxbench oei [--every 3] [--ncentre 30] [--reps 5]
 
 jk:  Coulomb and exchange matrices (simint_b200_basis_jk) of a seeded
      symmetric density from the FP64 sweep of every stride-th bra row of the
      l <= 3 workload basis (500 shells, s:p:d:f 200:150:100:50, 1-8
-     primitives, exponents 0.05-5e4, Schwarz 1e-14).
+     primitives, exponents 0.05-5e4, Schwarz 1e-14); beside it the sweep
+     alone and the sweep with its digestion through a scratch buffer of
+     scratch-mb MB (simint_b200_basis_compute_jk).
 oei: overlap, kinetic-energy and nuclear-attraction matrices
      (simint_b200_oei_matrix) of every `every`-th shell of the same basis over
      ncentre seeded point charges (Z = 6) in the basis' 20 bohr box.
@@ -51,7 +53,7 @@ def _time(torch, stream, fn, reps):
     return statistics.median(ms)
 
 
-def run_jk(stride=8000, reps=5):
+def run_jk(stride=8000, reps=5, scratch_mb=48):
     import torch
     lib = load()
     lib.simint_init()
@@ -69,8 +71,22 @@ def run_jk(stride=8000, reps=5):
     J, K = torch.empty_like(D), torch.empty_like(D)
     ms = _time(torch, st, lambda: B.jk(out.data_ptr(), n, D.data_ptr(), J.data_ptr(), K.data_ptr(),
                                        st.cuda_stream), reps)
+    # the sweep alone, and the sweep with its digestion through an L2-sized
+    # scratch buffer (the integrals never leave L2 for HBM)
+    ms_sweep = _time(torch, st, lambda: B.compute(FP64, out.data_ptr(), n, st.cuda_stream), reps)
+    cap = min(n, scratch_mb * (1 << 20) // 8)
+    scratch = torch.empty(max(cap, 1), dtype=torch.float64, device="cuda")
+    J2, K2 = torch.empty_like(D), torch.empty_like(D)
+    ms_fused = _time(torch, st, lambda: B.compute_jk(FP64, D.data_ptr(), J2.data_ptr(), K2.data_ptr(),
+                                                     scratch.data_ptr(), cap, st.cuda_stream), reps)
+    torch.cuda.synchronize()
+    dj = float((J2 - J).abs().max()) / max(float(J.abs().max()), 1e-300)
+    dk = float((K2 - K).abs().max()) / max(float(K.abs().max()), 1e-300)
     return {"what": "jk", "stride": stride, "nbf": nbf, "quartets": B.nquartets,
-            "integrals_mb": n * 8 / 1e6, "ms": ms, "integrals_gb_s": n * 8 / ms / 1e6}
+            "integrals_mb": n * 8 / 1e6, "ms": ms, "integrals_gb_s": n * 8 / ms / 1e6,
+            "sweep_ms": ms_sweep, "sweep_plus_jk_ms": ms_sweep + ms,
+            "compute_jk_ms": ms_fused, "scratch_mb": cap * 8 / 2 ** 20,
+            "compute_jk_vs_jk_rel": max(dj, dk)}
 
 
 def run_oei(every=3, ncentre=30, reps=5):
@@ -101,9 +117,10 @@ def main():
     ap.add_argument("--every", type=int, default=3)
     ap.add_argument("--ncentre", type=int, default=30)
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--scratch-mb", type=int, default=48)
     a = ap.parse_args()
     if a.what == "jk":
-        print(json.dumps(run_jk(a.stride, a.reps)))
+        print(json.dumps(run_jk(a.stride, a.reps, a.scratch_mb)))
     else:
         print(json.dumps(run_oei(a.every, a.ncentre, a.reps)))
 

@@ -69,6 +69,18 @@ def test_jk_matches_full_tensor(ordering, basis):
         B.jk(out.data_ptr(), n, dD.data_ptr(), dJ.data_ptr(), dK.data_ptr())
     torch.cuda.synchronize()
     J, K = dJ.cpu().numpy(), dK.cpu().numpy()
+    # the same digestion chunk by chunk through a small scratch buffer (one
+    # to a few quartets of the largest class per chunk), and through a
+    # scratch buffer that holds the whole sweep
+    nmax = max(c["nout"] for c in B.classes())
+    for cap in (nmax + 7, n):
+        scratch = torch.empty(cap, dtype=torch.float64, device="cuda")
+        dJ2, dK2 = torch.empty_like(dJ), torch.empty_like(dK)
+        B.compute_jk(sb.FP64, dD.data_ptr(), dJ2.data_ptr(), dK2.data_ptr(), scratch.data_ptr(), cap)
+        torch.cuda.synchronize()
+        # (atomic adds in another order: equal to rounding)
+        assert np.allclose(dJ2.cpu().numpy(), J, rtol=1e-13, atol=1e-13 * np.abs(J).max())
+        assert np.allclose(dK2.cpu().numpy(), K, rtol=1e-13, atol=1e-13 * np.abs(K).max())
     B.close()
     lib.simint_b200_set_ordering(0)
     scale = max(np.abs(J_ref).max(), np.abs(K_ref).max())
