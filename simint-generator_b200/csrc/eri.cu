@@ -840,6 +840,29 @@ struct CallTrace
 };
 } // namespace
 
+// Ket pairs c0 .. c1-1 of Q in decreasing primitive count, equal counts in
+// list order (a stable counting sort; a comparison sort for counts above
+// 4096), into out.
+static void kets_by_nprim(const simint_multi_shellpair * Q, int c0, int c1, int * out)
+{
+    int mx = 0;
+    for(int q = c0; q < c1; q++)
+        mx = std::max(mx, Q->nprim12[q]);
+    if(mx > 4096)
+    {
+        for(int q = c0; q < c1; q++) out[q - c0] = q;
+        std::stable_sort(out, out + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+        return;
+    }
+    std::vector<int> first(mx + 2, 0);
+    for(int q = c0; q < c1; q++)
+        first[mx - std::max(Q->nprim12[q], 0) + 1]++;
+    for(int v = 1; v <= mx + 1; v++)
+        first[v] += first[v - 1];
+    for(int q = c0; q < c1; q++)
+        out[first[mx - std::max(Q->nprim12[q], 0)]++] = q;
+}
+
 static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, const simint_multi_shellpair * Q,
                                  double screen_tol, double * integrals, int nc)
 {
@@ -947,8 +970,7 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         tr.time(tr.pack, [&] {
             if(!pinQ)
                 pack_records(Q, LQ.npad, g0, g1, (double *)hs);
-            for(int q = c0; q < c1; q++) kk[q - c0] = q;
-            std::stable_sort(kk, kk + (c1 - c0), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+            kets_by_nprim(Q, c0, c1, kk);
         });
         if(recbytes)
             cudaMemcpyAsync(d + szP + (size_t)g0 * SB_REC * sizeof(double), hs, recbytes, cudaMemcpyHostToDevice,
@@ -1044,8 +1066,7 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     const bool pinQ = pair_data_pinned(Q) && pair_arrays_in_block(Q, LQ.npad);
     // ket order: by primitive count (descending), stable
     std::vector<int> kord(Q->nshell12_clip);
-    for(int k = 0; k < Q->nshell12_clip; k++) kord[k] = k;
-    std::stable_sort(kord.begin(), kord.end(), [Q](int x, int y) { return Q->nprim12[x] > Q->nprim12[y]; });
+    kets_by_nprim(Q, 0, Q->nshell12_clip, kord.data());
     const size_t szK = (kord.size() * sizeof(int) + 255) & ~(size_t)255;
     if(!w.hstage.reserve(szP + szQ + szK) || !w.dpair.reserve(szP + szQ + szK))
     {
@@ -1102,9 +1123,10 @@ extern "C" int simint_compute_eri_deriv(int deriv,
     }
     int r = 0;
     // results through the pinned staging buffer (full-speed DMA; a copy
-    // into pageable memory would go through the driver's own staging), then
-    // into the caller's memory on all host cores
-    const bool staged = outbytes >= (64u << 10) && w.hout.reserve(outbytes);
+    // into pageable memory would go through the driver's own staging and
+    // return only when done), then into the caller's memory on the host
+    // threads
+    const bool staged = w.hout.reserve(outbytes);
     tr.time(tr.issue, [&] {
         tr.mark(0, w.stream);
         r = launch_rectangle(P, dP, Q, dQ, (const int *)(d + szP + szQ), screen_tol, deriv,

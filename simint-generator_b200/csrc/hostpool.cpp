@@ -116,10 +116,12 @@ void parallel_for(size_t n, size_t min_piece, const std::function<void(size_t, s
     p.fn = nullptr;
 }
 
+// 256 KB blocks, at least two per piece: a copy of a few MB already spreads
+// over most host threads (one thread copies about 10 GB/s)
 void parallel_copy(void * dst, const void * src, size_t bytes)
 {
-    const size_t blk = 1 << 20;
-    parallel_for((bytes + blk - 1) / blk, 4, [&](size_t lo, size_t hi) {
+    const size_t blk = 256 << 10;
+    parallel_for((bytes + blk - 1) / blk, 2, [&](size_t lo, size_t hi) {
         const size_t a = lo * blk, b = std::min(bytes, hi * blk);
         memcpy((char *)dst + a, (const char *)src + a, b - a);
     });
