@@ -336,11 +336,14 @@ int simint_b200_basis_jk(simint_b200_basis * b, const double * dev_out, long lon
                          const double * dev_D, double * dev_J, double * dev_K, void * stream);
 
 /* The sweep and its J/K digestion in one pass, without the sweep's output
- * in HBM: each class runs in chunks of scratch_doubles / (integrals per
- * quartet) shell quartets through dev_scratch, and each chunk is contracted
- * into J and K (as simint_b200_basis_jk) right after it is computed, on the
- * same stream, while its integrals are still in the 126 MB L2 (a scratch
- * buffer of a few tens of MB keeps them there).  prec as for
+ * in HBM: the classes run on four streams at once (as a full-layout sweep
+ * runs them), each stream streaming its classes in chunks through its
+ * quarter of dev_scratch, and each chunk is contracted into J and K (as
+ * simint_b200_basis_jk) right after it is computed, on the same stream,
+ * while its integrals are still in the 126 MB L2 (a scratch buffer of a few
+ * tens of MB keeps them there).  A scratch buffer whose quarter cannot hold
+ * one quartet of every class is used by one stream; one that holds the
+ * whole sweep is used as its full layout.  prec as for
  * simint_b200_basis_compute; the class checksums are accumulated as by a
  * streamed compute.  dev_scratch must hold one quartet of every class;
  * classes whose digestion does not fit shared memory return

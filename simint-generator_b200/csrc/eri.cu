@@ -448,11 +448,13 @@ bool pair_arrays_in_block(const simint_multi_shellpair * P, int npad)
 }
 
 // Pair set P (arrays in page-locked host memory) into the packed layout L at
-// dpack on `stream`: one DMA of its allocation into dsoa, the pair starts
-// from hstart (page-locked, start.size() ints, kept until the stream has
-// run), the records and metadata built on the device.
+// dpack on `stream`: the arrays the records need (2a and 2b only for
+// derivatives) into dsoa at their offsets in the allocation, one DMA per run
+// of adjacent arrays; the pair starts from hstart (page-locked,
+// start.size() ints, kept until the stream has run); the records and
+// metadata built on the device.
 int upload_pinned_pairs(const simint_multi_shellpair * P, const PackedLayout & L, const std::vector<int> & start,
-                        char * dpack, DevBuf & dsoa, int * hstart, cudaStream_t stream)
+                        char * dpack, DevBuf & dsoa, int * hstart, cudaStream_t stream, int deriv)
 {
     if(!dsoa.reserve(P->memsize))
     {
@@ -466,9 +468,33 @@ int upload_pinned_pairs(const simint_multi_shellpair * P, const PackedLayout & L
     o.pax = off(P->PA_x); o.pay = off(P->PA_y); o.paz = off(P->PA_z);
     o.pbx = off(P->PB_x); o.pby = off(P->PB_y); o.pbz = off(P->PB_z);
     o.alpha = off(P->alpha); o.prefac = off(P->prefac); o.screen = off(P->screen);
-    o.a2 = off(P->alpha2); o.b2 = off(P->beta2);
+    // 2a and 2b only weigh derivative integrals
+    o.a2 = deriv ? off(P->alpha2) : -1;
+    o.b2 = deriv ? off(P->beta2) : -1;
     o.abx = off(P->AB_x); o.aby = off(P->AB_y); o.abz = off(P->AB_z); o.nprim12 = off(P->nprim12);
-    cudaMemcpyAsync(dsoa.ptr, P->ptr, P->memsize, cudaMemcpyHostToDevice, stream);
+    // one DMA per run of adjacent arrays the records need
+    const size_t dprim = (size_t)L.npad * sizeof(double), dpair = (size_t)L.npair * sizeof(double);
+    std::vector<std::pair<long long, size_t>> r;
+    for(long long a : {o.x, o.y, o.z, o.pax, o.pay, o.paz, o.pbx, o.pby, o.pbz, o.alpha, o.prefac, o.screen,
+                       o.a2, o.b2})
+        if(a >= 0)
+            r.push_back({a, dprim});
+    for(long long a : {o.abx, o.aby, o.abz})
+        if(a >= 0)
+            r.push_back({a, dpair});
+    if(o.nprim12 >= 0)
+        r.push_back({o.nprim12, (size_t)L.npair * sizeof(int)});
+    std::sort(r.begin(), r.end());
+    for(size_t k = 0; k < r.size();)
+    {
+        long long a = r[k].first, e = a + (long long)r[k].second;
+        size_t m = k + 1;
+        for(; m < r.size() && r[m].first <= e; m++)
+            e = std::max(e, r[m].first + (long long)r[m].second);
+        cudaMemcpyAsync((char *)dsoa.ptr + a, (const char *)P->ptr + a, (size_t)(e - a), cudaMemcpyHostToDevice,
+                        stream);
+        k = m;
+    }
     memcpy(hstart, start.data(), (size_t)L.npair * sizeof(int));
     cudaMemcpyAsync(dpack + L.off_start, hstart, (size_t)L.npair * sizeof(int), cudaMemcpyHostToDevice, stream);
     k_soa_records<<<(unsigned)((L.npad + 255) / 256), 256, 0, stream>>>((const char *)dsoa.ptr, o, L.npad,
@@ -917,10 +943,10 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
     }
     // P, and Q's starts/counts/AB (everything after the records); a pinned
     // Q goes up whole, its records built on the device
-    int rc0 = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
+    int rc0 = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream, deriv)
                    : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
     if(rc0 == 0)
-        rc0 = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
+        rc0 = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream, deriv)
                    : (cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start,
                                       cudaMemcpyHostToDevice, w.stream), 0);
     if(rc0 != 0)
@@ -1099,10 +1125,11 @@ extern "C" int simint_compute_eri_deriv(int deriv,
                 return;
             }
             // the unused host staging of a pinned set holds its pair starts
-            rc_up = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream)
+            rc_up = pinP ? upload_pinned_pairs(P, LP, pstart, d, w.dsoa, (int *)h, w.stream, deriv)
                          : (cudaMemcpyAsync(d, h, szP, cudaMemcpyHostToDevice, w.stream), 0);
             if(rc_up == 0)
-                rc_up = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream)
+                rc_up = pinQ ? upload_pinned_pairs(Q, LQ, qstart, d + szP, w.dsoa, (int *)(h + szP), w.stream,
+                                                   deriv)
                              : (cudaMemcpyAsync(d + szP, h + szP, szQ, cudaMemcpyHostToDevice, w.stream), 0);
             if(rc_up == 0)
                 cudaMemcpyAsync(d + szP + szQ, h + szP + szQ, szK, cudaMemcpyHostToDevice, w.stream);

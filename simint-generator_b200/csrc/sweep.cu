@@ -1544,17 +1544,76 @@ extern "C" int simint_b200_basis_compute_jk(simint_b200_basis * b, int prec, con
     cudaMemsetAsync(b->dsums.ptr, 0, 2 * sizeof(double) * b->qcs.size(), stream);
     cudaMemsetAsync(b->dqueue.ptr, 0, SWEEP_QSTRIDE * b->qcs.size(), stream);
     const JKJob job = {dev_D, dev_J, dev_K};
-    // a scratch buffer that holds the whole sweep is used as such: each
-    // class writes its own range and is digested from there
     int nl = 0;
-    for(size_t k = 0; k < b->qcs.size(); k++)
+    long long maxout = 1;
+    for(const auto & q : b->qcs)
+        if(q.ntask > 0)
+            maxout = std::max<long long>(maxout, q.nout);
+    const int ns = SWEEP_SIDE + 1;
+    const long long part = scratch_doubles / ns;
+    if(scratch_doubles >= b->total_out || part < maxout)
     {
-        if(b->qcs[k].ntask == 0)
-            continue;
-        rc = issue_class(b, k, prec, dev_scratch, scratch_doubles, stream, &job);
+        // one stream: a scratch buffer that holds the whole sweep is used as
+        // the full layout (each class digested from its own range), a
+        // smaller one streams every class through it
+        for(size_t k = 0; k < b->qcs.size(); k++)
+        {
+            if(b->qcs[k].ntask == 0)
+                continue;
+            rc = issue_class(b, k, prec, dev_scratch, scratch_doubles, stream, &job);
+            if(rc < 0)
+                return rc;
+            nl += rc;
+        }
+    }
+    else
+    {
+        // the classes on SWEEP_SIDE + 1 streams at once, as a full-layout
+        // sweep runs them, each stream streaming its classes through its own
+        // part of the scratch buffer (J and K take atomic adds from all)
+        if(!b->fork)
+        {
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+            for(int i = 0; i < SWEEP_SIDE; i++)
+            {
+                cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+                cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+            }
+        }
+        std::vector<size_t> order(b->qcs.size());
+        std::iota(order.begin(), order.end(), 0);
+        auto cost = [&](size_t k) {
+            const QClass & q = b->qcs[k];
+            const int L = q.req[0] + q.req[1] + q.req[2] + q.req[3];
+            return (double)q.ntask * q.nout * (1.0 + L);
+        };
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return cost(x) > cost(y); });
+        double load[SWEEP_SIDE + 1] = {};
+        cudaEventRecord(b->fork, stream);
+        for(int i = 0; i < SWEEP_SIDE; i++)
+            cudaStreamWaitEvent(b->side[i], b->fork, 0);
+        for(size_t k : order)
+        {
+            if(b->qcs[k].ntask == 0)
+                continue;
+            int sidx = 0;
+            for(int i = 1; i <= SWEEP_SIDE; i++)
+                if(load[i] < load[sidx]) sidx = i;
+            load[sidx] += cost(k);
+            set_workspace_override(sidx ? &b->side_ws[sidx - 1] : nullptr);
+            rc = issue_class(b, k, prec, dev_scratch + sidx * part, part, sidx ? b->side[sidx - 1] : stream, &job);
+            set_workspace_override(nullptr);
+            if(rc < 0)
+                break;
+            nl += rc;
+        }
+        for(int i = 0; i < SWEEP_SIDE; i++)
+        {
+            cudaEventRecord(b->join[i], b->side[i]);
+            cudaStreamWaitEvent(stream, b->join[i], 0);
+        }
         if(rc < 0)
             return rc;
-        nl += rc;
     }
     rc = jk_finish(b, job, stream);
     return rc < 0 ? rc : nl + rc;

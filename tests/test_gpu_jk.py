@@ -70,10 +70,13 @@ def test_jk_matches_full_tensor(ordering, basis):
     torch.cuda.synchronize()
     J, K = dJ.cpu().numpy(), dK.cpu().numpy()
     # the same digestion chunk by chunk through a small scratch buffer (one
-    # to a few quartets of the largest class per chunk), and through a
-    # scratch buffer that holds the whole sweep
+    # to a few quartets of the largest class per chunk), through one split
+    # between the four class streams, and through a scratch buffer that
+    # holds the whole sweep
     nmax = max(c["nout"] for c in B.classes())
-    for cap in (nmax + 7, n):
+    # (one stream through nmax + 7 doubles; four streams through a quarter
+    # of 4 nmax + 64 each; the full layout)
+    for cap in (nmax + 7, 4 * nmax + 64, n):
         scratch = torch.empty(cap, dtype=torch.float64, device="cuda")
         dJ2, dK2 = torch.empty_like(dJ), torch.empty_like(dK)
         B.compute_jk(sb.FP64, dD.data_ptr(), dJ2.data_ptr(), dK2.data_ptr(), scratch.data_ptr(), cap)
