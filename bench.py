@@ -30,7 +30,8 @@ Workloads (--config; seeded synthetic shells of simint_b200/workloads.py):
 Metric: evaluated primitive quartets per second (after the reference's
 primitive screening).  `value` is device time with inputs resident in HBM;
 `e2e` the same metric through simint_compute_eri(_deriv) with host buffers
-(uploads and downloads inside the timed region); `cpu_baseline` the
+(uploads and downloads inside the timed region), the calls issued from up to
+16 host threads at once as the reference arm runs its rows; `cpu_baseline` the
 reference's generated CPU library (create.py output, gcc -O3, OpenMP over
 rows) on the same rows, timed on this machine's cores.  Sweep outputs are
 compared with the reference's values element by element (cfg1/2/3), by
@@ -77,6 +78,7 @@ def note(msg):
     print("[bench +%.1fs] %s" % (time.time() - T_START, msg), file=sys.stderr, flush=True)
 
 PSI4, GAMESS = 0, 1
+E2E_THREADS = min(16, os.cpu_count() or 1)   # host threads issuing the e2e calls
 LINE_LIMIT = 3000               # bytes of the printed result line (kept well under 4 KB)
 METRIC = "primitive quartets/s per AM class, mixed-prec vs FP64 on 1 B200 at ≤1e-10 abs err"
 
@@ -257,6 +259,31 @@ def sample_rows(sb, lib, S, B, every, screen):
                 quartets.append((first, sh4[first:first + n]))
             t += 1
     return rows, quartets
+
+
+def e2e_times(sb, fn, calls, steps, warmup, threads):
+    """Host seconds of each of `steps` passes over `calls` (argument tuples
+    of fn, a C-ABI call through ctypes, which releases the GIL), issued from
+    `threads` host threads at once, largest calls first -- the way an
+    OpenMP loop over bra pairs calls the reference (skel/test/test_eri.cpp
+    runs its rows in parallel), each thread with its own stream and buffers
+    inside the library.  `warmup` untimed passes first."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(args):
+        r = fn(*args)
+        if r < -1:
+            raise RuntimeError(sb.last_error())
+
+    with ThreadPoolExecutor(max_workers=threads) as pool:
+        for _ in range(max(1, warmup)):
+            list(pool.map(one, calls))
+        times = []
+        for _ in range(steps):
+            t = time.perf_counter()
+            list(pool.map(one, calls))
+            times.append(time.perf_counter() - t)
+    return times
 
 
 def free_rows(sb, lib, rows):
@@ -526,22 +553,16 @@ def run_b200(args):
                          * sb.ncart(Q.am1) * sb.ncart(Q.am2)) for _, _, P, Q in rows]
         d2h = sum(b.nbytes for b in bufs)
         dp = C.POINTER(C.c_double)
-        for _ in range(max(1, args.warmup)):
-            for (_, am, P, Q), buf in zip(rows, bufs):
-                lib.simint_compute_eri(C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-        times = []
-        for _ in range(args.steps):
-            t = time.perf_counter()
-            for (_, am, P, Q), buf in zip(rows, bufs):
-                r = lib.simint_compute_eri(C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-                if r < -1:
-                    raise RuntimeError(sb.last_error())
-            times.append(time.perf_counter() - t)
+        cost = [b.size for b in bufs]
+        calls = [(C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
+                 for _, (_, am, P, Q), buf in sorted(zip(cost, rows, bufs), key=lambda x: -x[0])]
+        nthr = max(1, min(len(calls), E2E_THREADS))
+        times = e2e_times(sb, lib.simint_compute_eri, calls, args.steps, args.warmup, nthr)
         lib.simint_b200_set_precision(sb.FP64, 0.0)
-        note("e2e: %d calls, %.1f ms per step" % (len(rows), 1e3 * statistics.median(times)))
+        note("e2e: %d calls on %d host threads, %.1f ms per step" % (len(rows), nthr, 1e3 * statistics.median(times)))
         e2e = {"value": npq_e2e / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "calls_per_step": len(rows), "primq_per_step": int(npq_e2e),
+               "calls_per_step": len(rows), "host_threads": nthr, "primq_per_step": int(npq_e2e),
                "precision": "mixed" if head_mixed else "fp64"}
         # the calls' results against the sweep's values of the same quartets
         # (each call's ket list holds only the row's kets, so the 8-wide
@@ -766,22 +787,15 @@ def run_b200_rows(args, torch, sb, lib, shells, S, rank, world, local, dist):
     if rank == 0:
         bufs = [np.empty(n) for n in nouts]
         dp = C.POINTER(C.c_double)
-        for _ in range(max(1, args.warmup)):
-            for (_, _, P, Q), buf in zip(rows, bufs):
-                lib.simint_compute_eri_deriv(1, C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-        times = []
-        for _ in range(args.steps):
-            t = time.perf_counter()
-            for (_, _, P, Q), buf in zip(rows, bufs):
-                r = lib.simint_compute_eri_deriv(1, C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-                if r < -1:
-                    raise RuntimeError(sb.last_error())
-            times.append(time.perf_counter() - t)
-        note("e2e: %.1f ms per step" % (1e3 * statistics.median(times)))
+        calls = [(1, C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
+                 for _, (_, _, P, Q), buf in sorted(zip([b.size for b in bufs], rows, bufs), key=lambda x: -x[0])]
+        nthr = max(1, min(len(calls), E2E_THREADS))
+        times = e2e_times(sb, lib.simint_compute_eri_deriv, calls, args.steps, args.warmup, nthr)
+        note("e2e: %d calls on %d host threads, %.1f ms per step" % (len(rows), nthr, 1e3 * statistics.median(times)))
         e2e = {"value": npq / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(sum(pack_bytes(P) + pack_bytes(Q) for _, _, P, Q in rows)),
                "d2h_bytes_per_step": int(sum(b.nbytes for b in bufs)), "calls_per_step": len(rows),
-               "precision": "fp64"}
+               "host_threads": nthr, "precision": "fp64"}
         reflib, refsweep, R = load_reference(w["ref"]) if not (args.no_cpu and args.no_check) \
             else (None, None, "")
         if reflib is not None:

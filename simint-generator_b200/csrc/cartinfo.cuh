@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 #include <array>
+#include <mutex>
 #include <vector>
 
 #include "simint_b200.h"
@@ -118,14 +119,20 @@ static std::vector<CartInfo> cart_table_host()
     return t;
 }
 
+// Once per device, under a lock: calls from several host threads may come
+// first at the same time.
 static void upload_cart_info()
 {
-    static int done_dev = -1;
+    static std::mutex m;
+    static std::vector<char> done;
     int dev = 0;
     cudaGetDevice(&dev);
-    if(done_dev == dev)
+    std::lock_guard<std::mutex> lk(m);
+    if((int)done.size() > dev && done[dev])
         return;
     const std::vector<CartInfo> t = cart_table_host();
     cudaMemcpyToSymbol(c_cartinfo, t.data(), sizeof(CartInfo) * CI_NCART);
-    done_dev = dev;
+    if((int)done.size() <= dev)
+        done.resize(dev + 1, 0);
+    done[dev] = 1;
 }

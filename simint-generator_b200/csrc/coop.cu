@@ -523,14 +523,14 @@ int launch_coop(KernArgs & a, const int req[4], int deriv, int mode, cudaStream_
     a.oidx = nullptr;
     const int threads = 128;
     const size_t smem = (size_t)g.smem_doubles * sizeof(double);
-    static bool attr_set[3] = {false, false, false};
-    if(!attr_set[mode])
-    {
+    // per process (the attribute holds for every device the kernel runs on
+    // in this context); idempotent, so concurrent first calls are harmless
+    static std::once_flag attr_once[3];
+    std::call_once(attr_once[mode], [mode] {
         if(mode == 0) cudaFuncSetAttribute(k_coop<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if(mode == 1) cudaFuncSetAttribute(k_coop<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if(mode == 2) cudaFuncSetAttribute(k_coop<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr_set[mode] = true;
-    }
+    });
     const int per_sm = std::max(1, std::min(8, (int)((220 * 1024) / std::max<size_t>(smem, 1))));
     long long grid = std::min<long long>(a.ntask, 148LL * per_sm);
     grid = std::max<long long>(grid, 1);

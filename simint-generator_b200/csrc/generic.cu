@@ -17,6 +17,7 @@
 
 #include <cuda_runtime.h>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -356,12 +357,16 @@ namespace sb200 {
 static int lev_off_h(int l) { return l <= 0 ? 0 : (l * (l + 1) * (l + 2)) / 6; }
 static int nc_h(int l) { return ((l + 1) * (l + 2)) / 2; }
 
+// Once per device, under a lock (concurrent first calls from several host
+// threads).
 static void upload_cart_table()
 {
-    static int done_dev = -1;
+    static std::mutex m;
+    static std::vector<char> done;
     int dev = 0;
     cudaGetDevice(&dev);
-    if(done_dev == dev)
+    std::lock_guard<std::mutex> lk(m);
+    if((int)done.size() > dev && done[dev])
         return;
     std::vector<CartInfo> t(GNCART);
     std::vector<std::array<int, 3>> cs;
@@ -395,7 +400,9 @@ static void upload_cart_table()
         }
     }
     cudaMemcpyToSymbol(c_cart, t.data(), sizeof(CartInfo) * GNCART);
-    done_dev = dev;
+    if((int)done.size() <= dev)
+        done.resize(dev + 1, 0);
+    done[dev] = 1;
 }
 
 static bool setup_class(const int am[4], int deriv, GenClass & g)
