@@ -611,6 +611,17 @@ extern "C" size_t simint_eri_workmem(int derorder, int maxam)
 
 namespace sb200 {
 
+// Untuned default: the register kernel while its contracted tops fit
+// registers (above ~200 accumulators it spills), else the column kernel with
+// 4 primitive quartets per batch where it covers the class (the autotuner's
+// usual choice for the large classes), else the cooperative kernel.
+static int default_variant(const int req[4], int deriv, const ClassKernels * k)
+{
+    if(k && k->ntop <= 200)
+        return VAR_STRAIGHT;
+    return col_supported(req, deriv, 81) ? 81 : VAR_COOP2;
+}
+
 // Launch the kernel of class req for the prepared arguments a (P, Q,
 // tasks or kord, ntask, check, tol2, out, nout filled by the caller).
 int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
@@ -637,9 +648,7 @@ int launch_class(KernArgs & a, const int req[4], int deriv, int mode, int prec,
         a.gate = 0.0;
     }
     if(v == VAR_DEFAULT)
-        // untuned default: the register kernel while its contracted tops fit
-        // registers (above ~200 accumulators it spills), else cooperative
-        v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
+        v = default_variant(req, deriv, k);
     // a small rectangle (one simint_compute_eri call) gives a thread-per-
     // quartet kernel a handful of CTAs: the warp-per-quartet form of the
     // same register kernel spreads it over 32x the threads
@@ -706,7 +715,7 @@ bool class_uses_queue(const int req[4], int deriv, int prec)
     if(v >= 100)
         v -= 100;
     if(v == VAR_DEFAULT)
-        v = (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
+        v = default_variant(req, deriv, k);
     if((v == VAR_STRAIGHT || v == VAR_STRAIGHT64) && k)
         return false;
     if((v == VAR_WARP || v == VAR_WARP64) && k && k->fnw[2][0])
