@@ -206,8 +206,7 @@ int simint_b200_basis_autotune(simint_b200_basis * b, int prec, double * dev_out
 
 /* The kernel variant chosen for a requested class (0 = untuned default: the
  * register kernel while its contracted results fit registers, else the
- * column kernel with 4 per batch where it covers the class (deriv 0, bra and
- * ket depth at most 6), else the cooperative kernel;
+ * cooperative kernel;
  * 1 = register kernel, 20+B / 40+B / 60+B = cooperative kernel with 256 /
  * 128 / 64 threads and batch B = 1, 2, 4, 8, 81 / 82 = column kernel with
  * 4 / 8 primitive quartets per batch, 83 = column kernel with 4 per batch

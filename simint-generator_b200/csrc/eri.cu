@@ -612,14 +612,13 @@ extern "C" size_t simint_eri_workmem(int derorder, int maxam)
 namespace sb200 {
 
 // Untuned default: the register kernel while its contracted tops fit
-// registers (above ~200 accumulators it spills), else the column kernel with
-// 4 primitive quartets per batch where it covers the class (the autotuner's
-// usual choice for the large classes), else the cooperative kernel.
+// registers (above ~200 accumulators it spills), else the cooperative kernel
+// (the column kernel runs where the autotuner or a caller chooses it).
 static int default_variant(const int req[4], int deriv, const ClassKernels * k)
 {
-    if(k && k->ntop <= 200)
-        return VAR_STRAIGHT;
-    return col_supported(req, deriv, 81) ? 81 : VAR_COOP2;
+    (void)req;
+    (void)deriv;
+    return (k && k->ntop <= 200) ? VAR_STRAIGHT : VAR_COOP2;
 }
 
 // Launch the kernel of class req for the prepared arguments a (P, Q,
