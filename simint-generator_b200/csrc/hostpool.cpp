@@ -99,14 +99,7 @@ void parallel_for(size_t n, size_t min_piece, const std::function<void(size_t, s
         fn(0, n);
         return;
     }
-    // one loop at a time on the pool; a call that finds it busy (another
-    // host thread's simint_compute_eri) runs its loop on its own thread
-    std::unique_lock<std::mutex> call(p.call_m, std::try_to_lock);
-    if(!call.owns_lock())
-    {
-        fn(0, n);
-        return;
-    }
+    std::lock_guard<std::mutex> call(p.call_m);
     {
         std::lock_guard<std::mutex> lk(p.m);
         p.fn = &fn;

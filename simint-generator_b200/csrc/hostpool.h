@@ -10,8 +10,7 @@ namespace sb200 {
 
 // Run fn(lo, hi) over [0, n) split into contiguous pieces on the pool's
 // threads and the caller; returns when all pieces are done.  Small n runs
-// inline, and so does a call made while another host thread's loop holds the
-// pool (concurrent simint_compute_eri calls each copy on their own thread).
+// inline.  Calls from several host threads are serialised.
 void parallel_for(size_t n, size_t min_piece, const std::function<void(size_t, size_t)> & fn);
 
 // memcpy on the pool for large sizes.
