@@ -15,6 +15,9 @@
 
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <csignal>
+#include <execinfo.h>
+#include <unistd.h>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -550,9 +553,29 @@ using namespace sb200;
 // C API
 // =====================================================================
 
+// Opt-in crash report (SIMINT_B200_SEGV_TRACE=1): a segmentation fault in
+// any thread prints that thread's call stack (addresses inside the loaded
+// libraries) on stderr before the process ends as it would have.
+static void segv_report(int sig)
+{
+    void * frames[64];
+    const int n = backtrace(frames, 64);
+    static const char msg[] = "simint_b200: fatal signal, call stack:\n";
+    if(write(2, msg, sizeof(msg) - 1) < 0) {}
+    backtrace_symbols_fd(frames, n, 2);
+    signal(sig, SIG_DFL);
+    raise(sig);
+}
+
 extern "C" void simint_init(void)
 {
     init_tables();
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char * e = getenv("SIMINT_B200_SEGV_TRACE");
+        if(e && atoi(e) != 0)
+            signal(SIGSEGV, segv_report);
+    });
 }
 
 extern "C" void simint_finalize(void)

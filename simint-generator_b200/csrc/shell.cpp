@@ -352,6 +352,11 @@ extern "C" {
 void simint_fill_multi_shellpair2(int npair, struct simint_shell const * AB,
                                   struct simint_multi_shellpair * P, int screen_method)
 {
+    // pair sets are filled one at a time in the process (set-up work; the
+    // Schwarz values of a screened fill create a pair set of their own, so
+    // the lock is recursive)
+    static std::recursive_mutex fill_mutex;
+    std::lock_guard<std::recursive_mutex> fill_lock(fill_mutex);
     if(fill_on_gpu(npair, AB))
     {
         const int rc = sb200::gpu_fill_multi_shellpair2(npair, AB, P, screen_method);
