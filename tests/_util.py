@@ -129,3 +129,27 @@ class RowLD:
         self.orc.oracle_free_pair(C.byref(P))
         self.orc.oracle_free_pair(C.byref(Q))
         return out
+
+
+def in_child_process(fn):
+    """Run a test in a child pytest process (the same test id), so that a
+    crash of the process -- these tests drive both libraries from 16 OpenMP
+    threads of a C driver -- fails that test alone instead of ending the
+    whole session.  The child runs the body itself (SB_TEST_CHILD=1)."""
+    import functools
+    import os
+    import subprocess
+    import sys
+
+    @functools.wraps(fn)
+    def wrapper(*args, **kwargs):
+        if os.environ.get("SB_TEST_CHILD") == "1":
+            return fn(*args, **kwargs)
+        node = os.environ.get("PYTEST_CURRENT_TEST", "").rsplit(" ", 1)[0]
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        env = dict(os.environ, SB_TEST_CHILD="1")
+        r = subprocess.run([sys.executable, "-m", "pytest", node, "-q", "-p", "no:cacheprovider", "-x"],
+                           cwd=root, env=env, capture_output=True, text=True, timeout=1500)
+        out = (r.stdout + r.stderr)[-4000:]
+        assert r.returncode == 0, "child pytest for %s ended with %d:\n%s" % (node, r.returncode, out)
+    return wrapper

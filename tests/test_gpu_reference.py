@@ -42,7 +42,7 @@ import reflib
 import refsweep
 from simint_b200.workloads import config_shells
 from oracle import load_oracle, load_oracle_ld
-from _util import parity_bad, quartets_unexplained, RowLD, NC
+from _util import parity_bad, quartets_unexplained, RowLD, NC, in_child_process
 
 pytestmark = pytest.mark.gpu
 
@@ -109,6 +109,7 @@ def run_rows(D, shells, pairs, keys, cls, rows, ordering_lib=None, threads=None)
     return ret, out
 
 
+@in_child_process
 def test_cfg1_all_quartets_gamess(lib, drv):
     R = need("gamess_l3")
     shells = config_shells("cfg1")
@@ -197,6 +198,7 @@ def check_rows(S, shells, calc, ref, tol, deriv, ordering):
     return nq, nover
 
 
+@in_child_process
 def test_cfg2_rows_gamess(lib, drv):
     shells = config_shells("cfg2")
     S, ref, calc = sweep_case(lib, drv, "gamess_l3", shells, 1e-14, 3, 997, sb.GAMESS)
@@ -205,6 +207,7 @@ def test_cfg2_rows_gamess(lib, drv):
     assert nover <= 1e-4 * nq, (nover, nq)
 
 
+@in_child_process
 def test_cfg5_rows_psi4(lib, drv):
     shells = config_shells("cfg5")[::8]
     S, ref, calc = sweep_case(lib, drv, "psi4_l4", shells, 1e-12, 4, 211, sb.PSI4)
@@ -213,6 +216,7 @@ def test_cfg5_rows_psi4(lib, drv):
     assert nover <= 1e-3 * nq, (nover, nq)
 
 
+@in_child_process
 def test_cfg4_deriv1_rows_psi4(lib, drv):
     shells = config_shells("cfg4")
     S, ref, calc = sweep_case(lib, drv, "psi4_d1_l2", shells, 1e-14, 2, 401, sb.PSI4, deriv=1)
@@ -224,6 +228,7 @@ def test_cfg4_deriv1_rows_psi4(lib, drv):
     assert nover <= 3e-3 * nq, (nover, nq)
 
 
+@in_child_process
 def test_cfg4_deriv1_finite_differences(lib, drv):
     """Analytic gradients of our FP64 path against central differences of
     our FP64 ERIs: each centre of a quartet moved by +-h along x, y, z
@@ -283,6 +288,7 @@ def _fixture_cases(path):
 
 
 @pytest.mark.parametrize("fname,deriv", [("valeev_fg.npz", 0), ("valeev_fg_d1.npz", 1)])
+@in_child_process
 def test_gpu_matches_valeev_fg(lib, drv, fname, deriv):
     """Our GPU path against ValeevRef (the reference's long-double oracle)
     on f and g classes at the configurations' exponent range: the
@@ -382,6 +388,7 @@ def sweep_quartets_unexplained(ref_out, ref_keys, ref_offs, vals, sh4, nout, nsh
     return out
 
 
+@in_child_process
 def test_sweep_against_reference(lib):
     """The batched sweep (simint_b200_basis_*, FP64 and mixed) on every 4th
     shell of cfg2, the whole screened sweep:
