@@ -310,12 +310,17 @@ void pair_starts(const simint_multi_shellpair * P, std::vector<int> & start, int
 
 // Pack one pair set into host staging memory: records, starts, counts, AB.
 // Records of padded slots [g0, g1) (multiples of 8, the vector-screening
-// groups) into rec (slot 0 of rec = slot g0), on the host pool.
+// groups) into rec (slot 0 of rec = slot g0), on the calling thread (pair
+// sets large enough for packing to matter are page-locked and go up by DMA;
+// a calling thread's packing on the shared host pool died in pool threads
+// under a C driver's row loop, cause not found).
 void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, double * rec)
 {
     const bool has_screen = P->screen != nullptr;
     g1 = std::min(g1, npad);
-    parallel_for((size_t)(g1 - g0 + 7) / 8, 256, [&](size_t b0, size_t b1) {
+    if(g1 <= g0)
+        return;
+    auto body = [&](size_t b0, size_t b1) {
         for(int g = g0 + (int)b0 * 8; g < std::min(g0 + (int)b1 * 8, g1); g += 8)
         {
             double m = 0.0;
@@ -337,7 +342,8 @@ void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, do
             for(int s = g; s < ge; s++)
                 rec[(size_t)(s - g0) * SB_REC + 14] = m;
         }
-    });
+    };
+    body(0, (size_t)(g1 - g0 + 7) / 8);
 }
 
 // Layout of the packed pair set: records, then starts, counts and AB at
