@@ -311,9 +311,7 @@ void pair_starts(const simint_multi_shellpair * P, std::vector<int> & start, int
 // Pack one pair set into host staging memory: records, starts, counts, AB.
 // Records of padded slots [g0, g1) (multiples of 8, the vector-screening
 // groups) into rec (slot 0 of rec = slot g0), on the calling thread (pair
-// sets large enough for packing to matter are page-locked and go up by DMA;
-// a calling thread's packing on the shared host pool died in pool threads
-// under a C driver's row loop, cause not found).
+// sets large enough for packing to matter are page-locked and go up by DMA).
 void pack_records(const simint_multi_shellpair * P, int npad, int g0, int g1, double * rec)
 {
     const bool has_screen = P->screen != nullptr;
