@@ -403,8 +403,8 @@ def test_sweep_against_reference(lib):
       (ff|ff)); a sample of them is judged against the long-double
       evaluation;
     * the rows of the simint_compute_eri calls under the same rules, and
-      equal to the sweep's rows except on quartets that the reference bar
-      marks ill-conditioned: a call of fewer than 16 384 quartets runs the
+      within the FP64 bar of the sweep's rows except on quartets that the
+      reference bar marks ill-conditioned: a call of fewer than 16 384 quartets runs the
       warp-per-quartet form of a register kernel, which sums the primitive
       contributions in another order than the sweep's thread-per-quartet
       form, and on those quartets the order shows (1.8e-10 on a cfg2 (ff|ss)
@@ -485,14 +485,16 @@ def test_sweep_against_reference(lib):
             unexplained = sweep_quartets_unexplained(ref_out, keys, offs, vals, sh4, c["nout"],
                                                      len(shells), ld, sample)
             assert not unexplained, (c["am"], ma, mr, unexplained[:3])
-        # the calls' rows equal the sweep's except on ill-conditioned quartets
-        # (of those the reference rows cover)
+        # the calls' rows agree with the sweep's within the FP64 bar (their
+        # kernels differ: warp against thread per quartet, so the rounding
+        # differs) except on ill-conditioned quartets (of those the
+        # reference rows cover)
         nq_out = c["nout"]
         matched = set(int(q) for q in _sweep_match(keys, sh4, len(shells))[2])
         for q in sorted(called[k] & matched):
             g = h64[a + q * nq_out:a + (q + 1) * nq_out]
             r = hcall[a + q * nq_out:a + (q + 1) * nq_out]
-            if np.abs(g - r).max() > 1e-14 * max(1.0, float(np.abs(r).max())):
+            if len(parity_bad(g, r)[0]):
                 assert q in qbad, (c["am"], q, float(np.abs(g - r).max()))
     assert ncmp > 100000
     B.close()
