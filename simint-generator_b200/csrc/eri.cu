@@ -985,13 +985,17 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
                    : (cudaMemcpyAsync(d + szP + LQ.off_start, h + szP + LQ.off_start, szQ - LQ.off_start,
                                       cudaMemcpyHostToDevice, w.stream), 0);
     if(rc0 != 0)
+    {
+        cudaStreamSynchronize(w.stream);
         return rc0;
+    }
     const PairSetDev dP = device_view(d, LP, P->screen_max);
     const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
     int * dkord = (int *)(d + szP + szQ);
     if(!w.dstream && cudaStreamCreateWithFlags(&w.dstream, cudaStreamNonBlocking) != cudaSuccess)
     {
         set_error("cudaStreamCreate failed");
+        cudaStreamSynchronize(w.stream);
         return SIMINT_B200_ERR_CUDA;
     }
     static thread_local std::vector<cudaEvent_t> ev;
@@ -1002,6 +1006,7 @@ static int compute_eri_pipelined(int deriv, const simint_multi_shellpair * P, co
         if(cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
         {
             set_error("cudaEventCreate failed");
+            cudaStreamSynchronize(w.stream);
             return SIMINT_B200_ERR_CUDA;
         }
         ev.push_back(e);
@@ -1173,7 +1178,12 @@ extern "C" int simint_compute_eri_deriv(int deriv,
             cudaMemcpyAsync(d, h, szP + szQ + szK, cudaMemcpyHostToDevice, w.stream);
     });
     if(rc_up != 0)
+    {
+        // copies already queued read the staging buffer: let them finish
+        // before the next call reuses it
+        cudaStreamSynchronize(w.stream);
         return rc_up;
+    }
     const PairSetDev dP = device_view(d, LP, P->screen_max);
     const PairSetDev dQ = device_view(d + szP, LQ, Q->screen_max);
     const int nc = ncart(P->am1) * ncart(P->am2) * ncart(Q->am1) * ncart(Q->am2) * (deriv ? 12 : 1);
@@ -1200,7 +1210,10 @@ extern "C" int simint_compute_eri_deriv(int deriv,
         tr.mark(2, w.stream);
     });
     if(r < 0)
+    {
+        cudaStreamSynchronize(w.stream);
         return r;
+    }
     cudaError_t e = cudaSuccess;
     tr.time(tr.wait, [&] { e = cudaStreamSynchronize(w.stream); });
     if(e == cudaSuccess)
