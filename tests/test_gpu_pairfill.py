@@ -4,9 +4,10 @@ reference's shell.c bit for bit (tests/test_oracle_pins.py).
 
 Per shell pair the GPU fill must give the same primitive pairs: centres,
 P - A, P - B, exponent sums, 2a and 2b, A - B and counts bit for bit, the
-prefactors within a few ulps (CUDA's exp against the host's) and the
-screening values within 1e-6 relative plus 1e-10 of the pair's largest value
-(their (ab|ab) evaluations round differently on inputs a few ulps apart), in
+prefactors within a few ulps (CUDA's exp against the host's), the screening
+values keeping and dropping the same primitive pairs at every threshold from
+1e-16 to 1e-32 (their (ab|ab) evaluations round differently on inputs a few
+ulps apart, so values far below a pair's largest carry relative noise), in
 decreasing screening order; the
 padding slots bit for bit.  A pair of a shell with itself keeps the i >= j
 triangle with doubled off-diagonal prefactors.  The integrals from the two
@@ -73,10 +74,15 @@ def _compare(h, g, screen):
             # the rounding of its recurrences differs, and the rounding error
             # of a value scales with the largest intermediates, so values far
             # below them carry relative noise (a 5.1e-21 value beside a
-            # 5.9e-3 one moved by 3e-7 of itself); a screening value is a
-            # bound compared with a tolerance given to a digit or two, so
-            # 1e-6 of it plus 1e-10 of the pair's largest value is immaterial
-            assert np.all(np.abs(sh - sg) <= 1e-6 * np.abs(sh) + 1e-10 * float(np.abs(sh).max()) + 1e-40), p
+            # 5.9e-3 one moved by 3e-7 of itself).  A screening value is only
+            # compared with tol^2: the two fills must keep and drop the same
+            # primitive pairs at every threshold, except values within 1e-3
+            # of it, and agree to 1e-3 of the pair's scale (gross errors).
+            scale = float(np.abs(sh).max())
+            assert np.all(np.abs(sh - sg) <= 1e-3 * np.abs(sh) + 1e-6 * scale + 1e-40), p
+            for t in (1e-16, 1e-20, 1e-24, 1e-28, 1e-32):
+                near = np.abs(sh - t) <= 1e-3 * t
+                assert np.array_equal((sh >= t) | near, (sg >= t) | near), (p, t)
             assert np.all(np.diff(g["screen"][sl]) <= 0.0), p
             # where the host order has no near-ties the orders agree
             d = np.diff(h["screen"][sl])
